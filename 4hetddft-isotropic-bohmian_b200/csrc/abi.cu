@@ -1,0 +1,617 @@
+// abi.cu -- the extern "C" entry points of include/he4_tddft.h.
+#include <math.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "common.cuh"
+
+namespace he4 {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+static bool valid_n(int n) {
+  // grid sizes accepted by the reference (tstgrid.f90:8-12)
+  static const int nv[52] = {1,   2,   3,   4,   5,   6,   8,   9,   10,  12,  15,  16,  18,
+                             20,  24,  25,  27,  30,  32,  36,  40,  45,  48,  50,  54,  60,
+                             64,  72,  75,  80,  81,  90,  96,  100, 108, 120, 125, 128, 135,
+                             144, 150, 160, 162, 180, 192, 200, 216, 225, 240, 243, 250, 256};
+  for (int i = 0; i < 52; i++)
+    if (nv[i] == n) return true;
+  return false;
+}
+
+static int check_params(const he4_params *p) {
+  if (!valid_n(p->nx) || !valid_n(p->ny) || !valid_n(p->nz)) {
+    set_error("grid %dx%dx%d: every size must be a valid FFT size <= 256 (tstgrid)", p->nx, p->ny, p->nz);
+    return HE4_E_ARG;
+  }
+  if (p->nx < 8 || p->ny < 8 || p->nz < 8) {
+    set_error("grid sizes below 8 are not supported");
+    return HE4_E_UNSUPPORTED;
+  }
+  if (p->npd < 3 || p->npd > 25 || p->npd % 2 == 0) {
+    set_error("npd=%d must be odd in [3,25]", p->npd);
+    return HE4_E_ARG;
+  }
+  if (p->npd > p->nx || p->npd > p->ny || p->npd > p->nz) {
+    set_error("npd=%d exceeds a grid dimension", p->npd);
+    return HE4_E_ARG;
+  }
+  if (p->icon != 8) {
+    set_error("icon=%d: only periodic boundary conditions (icon=8) are implemented", p->icon);
+    return HE4_E_UNSUPPORTED;
+  }
+  if (p->core4 != HE4_CORE_OT && p->core4 != HE4_CORE_OTC) {
+    set_error("core4=%d is not supported", p->core4);
+    return HE4_E_UNSUPPORTED;
+  }
+  if (p->n_par < 1 || p->n_par > (1 << 24)) {
+    set_error("n_par=%d out of range", p->n_par);
+    return HE4_E_ARG;
+  }
+  if (p->ironx < 0 || p->mimpur <= 0.0 || !(p->xmax > 0) || !(p->ymax > 0) || !(p->zmax > 0)) {
+    set_error("invalid ironx, mimpur or box size");
+    return HE4_E_ARG;
+  }
+  if (p->pot_kind != HE4_POT_TABLE && p->pot_kind != HE4_POT_MORSE && p->pot_kind != HE4_POT_NULL) {
+    set_error("unknown pot_kind %d", p->pot_kind);
+    return HE4_E_ARG;
+  }
+  if (p->precision != HE4_PREC_FP64) {
+    set_error("precision mode %d is not implemented", p->precision);
+    return HE4_E_UNSUPPORTED;
+  }
+  return HE4_OK;
+}
+
+template <typename T>
+static int dalloc(T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc of %zu bytes: %s", sizeof(T) * n, cudaGetErrorString(e));
+    *p = nullptr;
+    return HE4_E_NOMEM;
+  }
+  return HE4_OK;
+}
+
+static void free_all(Handle *h) {
+  fft_plan_free(h->fft);
+  void *ptrs[] = {h->wcgk, h->fvlj4, h->kalfs, h->vq, h->pmod, h->dsym, h->timec_re, h->psi, h->psiold[0],
+                  h->psiold[1], h->psiold[2], h->hpsiold[0], h->hpsiold[1], h->pc, h->q, h->ctmp, h->den, h->pot4,
+                  h->dencg, h->delj4, h->denalf, h->ualphas, h->falfs, h->intx, h->inty, h->intz, h->dxden,
+                  h->dyden, h->dzden, h->penalty, h->corr, h->denx, h->psix, h->hpsix, h->uimp, h->fx, h->fy,
+                  h->fz, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], h->counts, h->rimp, h->vimp, h->aimp,
+                  h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal};
+  for (void *p : ptrs) cudaFree(p);
+  for (int i = 0; i < 8; i++) cudaFree(h->spec[i]);
+  if (h->hscal) cudaFreeHost(h->hscal);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+static int create(const he4_params *pin, Handle *h) {
+  HE4_TRY(check_params(pin));
+  h->p = *pin;
+  h->p.vq_table = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return HE4_E_NODEVICE;
+  }
+  if (pin->device < 0 || pin->device >= ndev) {
+    set_error("device %d out of range (%d devices)", pin->device, ndev);
+    return HE4_E_ARG;
+  }
+  h->dev = pin->device;
+  HE4_CUDA_TRY(cudaSetDevice(h->dev));
+  cudaDeviceProp prop;
+  HE4_CUDA_TRY(cudaGetDeviceProperties(&prop, h->dev));
+  if (prop.major < 10) {
+    set_error("device %d (%s, sm_%d%d) is not an sm_100 GPU", h->dev, prop.name, prop.major, prop.minor);
+    return HE4_E_NODEVICE;
+  }
+  HE4_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  const he4_params &p = h->p;
+  h->nx = p.nx;
+  h->ny = p.ny;
+  h->nz = p.nz;
+  h->nxh = p.nx / 2 + 1;
+  h->npar = p.n_par;
+  h->N = (size_t)p.nx * p.ny * p.nz;
+  h->H = (size_t)h->nxh * p.ny * p.nz;
+  h->hx = 2.0 * fabs(p.xmax) / p.nx;
+  h->hy = 2.0 * fabs(p.ymax) / p.ny;
+  h->hz = 2.0 * fabs(p.zmax) / p.nz;
+  h->dxyz = h->hx * h->hy * h->hz;
+  h->renor = 1.0 / ((double)p.nx * p.ny * p.nz);
+  h->mAg_u = p.mimpur * 0.0206149591055;  // mp_u (modules.f90:314)
+  h->h2o2mx = p.h2o2m4 * (4.002602 / p.mimpur);
+  const size_t N = h->N, H = h->H, P3 = 3 * (size_t)h->npar;
+  HE4_TRY(fft_plan_init(h->fft, p.nx, p.ny, p.nz));
+  HE4_TRY(dalloc(&h->wcgk, H));
+  HE4_TRY(dalloc(&h->fvlj4, H));
+  HE4_TRY(dalloc(&h->kalfs, H));
+  HE4_TRY(dalloc(&h->vq, H));
+  HE4_TRY(dalloc(&h->pmod, H));
+  HE4_TRY(dalloc(&h->dsym, (size_t)p.nx + p.ny + p.nz));
+  HE4_TRY(dalloc(&h->timec_re, (size_t)p.nz));
+  double2 **cfields[] = {&h->psi, &h->psiold[0], &h->psiold[1], &h->psiold[2], &h->hpsiold[0],
+                         &h->hpsiold[1], &h->pc, &h->q, &h->ctmp};
+  for (double2 **f : cfields) HE4_TRY(dalloc(f, N));
+  double **rfields[] = {&h->den, &h->pot4, &h->dencg, &h->delj4, &h->denalf, &h->ualphas, &h->falfs,
+                        &h->intx, &h->inty, &h->intz, &h->dxden, &h->dyden, &h->dzden, &h->penalty,
+                        &h->corr, &h->denx, &h->psix, &h->hpsix, &h->uimp, &h->fx, &h->fy, &h->fz,
+                        &h->rtmp[0], &h->rtmp[1], &h->rtmp[2], &h->rtmp[3]};
+  for (double **f : rfields) HE4_TRY(dalloc(f, N));
+  HE4_TRY(dalloc(&h->counts, N));
+  for (int i = 0; i < 4; i++) HE4_TRY(dalloc(&h->spec[i], H));
+  double **pfields[] = {&h->rimp, &h->vimp, &h->aimp, &h->rimpold[0], &h->rimpold[1], &h->rimpold[2],
+                        &h->vimpold[0], &h->vimpold[1], &h->vimpold[2], &h->aimpold[0], &h->aimpold[1],
+                        &h->qr, &h->qv, &h->pcr, &h->pcv};
+  for (double **f : pfields) HE4_TRY(dalloc(f, P3));
+  // per-CTA partial sums of the grid reductions (7 energy sums max)
+  const size_t nblocks = (size_t)((p.nx + 31) / 32) * ((p.ny + 7) / 8) * p.nz;
+  h->red_len = 8 * nblocks;
+  HE4_TRY(dalloc(&h->red, h->red_len));
+  HE4_TRY(dalloc(&h->scal, 64));
+  HE4_CUDA_TRY(cudaMallocHost((void **)&h->hscal, 64 * sizeof(double)));
+  // the histories start at zero (dimen.f90:75-79,133-134; DFT4He3d.f90:841-845)
+  for (double2 **f : cfields) HE4_CUDA_TRY(cudaMemsetAsync(*f, 0, sizeof(double2) * N, h->stream));
+  for (double **f : rfields) HE4_CUDA_TRY(cudaMemsetAsync(*f, 0, sizeof(double) * N, h->stream));
+  for (double **f : pfields) HE4_CUDA_TRY(cudaMemsetAsync(*f, 0, sizeof(double) * P3, h->stream));
+  he4_params with_table = p;
+  with_table.vq_table = pin->vq_table;
+  h->p = with_table;
+  int e = setup_kernels(h);
+  h->p.vq_table = nullptr;
+  HE4_TRY(e);
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+}  // namespace he4
+
+using namespace he4;
+
+extern "C" {
+
+void he4_params_default(he4_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->nx = p->ny = p->nz = 64;
+  p->xmax = p->ymax = p->zmax = 64.0;
+  p->npd = 7;
+  p->icon = 8;
+  p->core4 = HE4_CORE_OT;
+  p->cp4 = -2.41186e4;
+  p->cpp4 = 1.85850e6;
+  p->den4c = 0.062;
+  p->alphas = 54.31;
+  p->l_alfs = 1.0;
+  p->den0s = 0.04;
+  p->h2o2m4 = 6.05969638298;
+  p->c_solid = 3.1577504e4;
+  p->beta_solid = 40.0;
+  p->den_m = 0.37;
+  p->eps4 = 10.22;
+  p->sigma4 = 2.556;
+  p->b4 = -718.99;
+  p->h4 = 2.190323;
+  p->n_par = 100000;
+  p->ironx = 1;
+  p->mimpur = 4.002602;
+  p->pot_kind = HE4_POT_NULL;
+  p->r_cutoff = 3.0;
+  p->umax = 400.0;
+  p->nq = 1000;
+  p->lambdah = 0.0;
+  p->tzmean = 0.0;
+  p->tzsurf = 1.0;
+  p->precision = HE4_PREC_FP64;
+  p->device = 0;
+}
+
+int he4_create(const he4_params *p, he4_handle **out) {
+  if (!p || !out) {
+    set_error("null argument");
+    return HE4_E_ARG;
+  }
+  *out = nullptr;
+  he4_handle *hh = new (std::nothrow) he4_handle();
+  if (!hh) {
+    set_error("host allocation failed");
+    return HE4_E_NOMEM;
+  }
+  int e = create(p, &hh->h);
+  if (e != HE4_OK) {
+    free_all(&hh->h);
+    delete hh;
+    return e;
+  }
+  *out = hh;
+  return HE4_OK;
+}
+
+void he4_destroy(he4_handle *hh) {
+  if (!hh) return;
+  cudaSetDevice(hh->h.dev);
+  if (hh->h.stream) cudaStreamSynchronize(hh->h.stream);
+  free_all(&hh->h);
+  delete hh;
+}
+
+#define HANDLE_OR_FAIL(hh)                 \
+  if (!(hh)) {                             \
+    set_error("null handle");              \
+    return HE4_E_ARG;                      \
+  }                                        \
+  Handle *h = &(hh)->h;                    \
+  if (cudaSetDevice(h->dev) != cudaSuccess) { \
+    set_error("cudaSetDevice failed");     \
+    return HE4_E_CUDA;                     \
+  }
+
+#define NEED_STATE(h)                                   \
+  if (!(h)->have_state) {                               \
+    set_error("no state: call he4_set_state first");    \
+    return HE4_E_STATE;                                 \
+  }
+
+int he4_set_state(he4_handle *hh, const double *psi, const double *rimp, const double *vimp) {
+  HANDLE_OR_FAIL(hh);
+  if (!psi || !rimp || !vimp) {
+    set_error("null state array");
+    return HE4_E_ARG;
+  }
+  const size_t N = h->N, P3 = 3 * (size_t)h->npar;
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->psi, psi, sizeof(double2) * N, cudaMemcpyHostToDevice, h->stream));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->rimp, rimp, sizeof(double) * P3, cudaMemcpyHostToDevice, h->stream));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->vimp, vimp, sizeof(double) * P3, cudaMemcpyHostToDevice, h->stream));
+  HE4_CUDA_TRY(cudaMemsetAsync(h->aimp, 0, sizeof(double) * P3, h->stream));
+  double2 *cz[] = {h->psiold[0], h->psiold[1], h->psiold[2], h->hpsiold[0], h->hpsiold[1], h->pc, h->q};
+  for (double2 *f : cz) HE4_CUDA_TRY(cudaMemsetAsync(f, 0, sizeof(double2) * N, h->stream));
+  double *pz[] = {h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv};
+  for (double *f : pz) HE4_CUDA_TRY(cudaMemsetAsync(f, 0, sizeof(double) * P3, h->stream));
+  for (int i = 0; i < 3; i++) h->ioldp[i] = h->ioldr[i] = h->ioldv[i] = i;
+  for (int i = 0; i < 2; i++) h->ioldh[i] = h->iolda[i] = i;
+  HE4_TRY(compute_den(h));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->have_state = 1;
+  h->nsteps_done = 0;
+  return HE4_OK;
+}
+
+int he4_get_state(he4_handle *hh, double *psi, double *rimp, double *vimp, double *aimp) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  const size_t P3 = 3 * (size_t)h->npar;
+  if (psi) HE4_CUDA_TRY(cudaMemcpyAsync(psi, h->psi, sizeof(double2) * h->N, cudaMemcpyDeviceToHost, h->stream));
+  if (rimp) HE4_CUDA_TRY(cudaMemcpyAsync(rimp, h->rimp, sizeof(double) * P3, cudaMemcpyDeviceToHost, h->stream));
+  if (vimp) HE4_CUDA_TRY(cudaMemcpyAsync(vimp, h->vimp, sizeof(double) * P3, cudaMemcpyDeviceToHost, h->stream));
+  if (aimp) HE4_CUDA_TRY(cudaMemcpyAsync(aimp, h->aimp, sizeof(double) * P3, cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+static int sync_and_check(Handle *h) {
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+int he4_potenimp(he4_handle *hh) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  HE4_TRY(field_potenimp(h));
+  return sync_and_check(h);
+}
+
+int he4_poten(he4_handle *hh) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  HE4_TRY(field_poten(h));
+  return sync_and_check(h);
+}
+
+int he4_forceimp(he4_handle *hh) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  HE4_TRY(field_forceimp(h));
+  return sync_and_check(h);
+}
+
+int he4_field(he4_handle *hh) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  HE4_TRY(field_potenimp(h));
+  HE4_TRY(field_poten(h));
+  HE4_TRY(field_forceimp(h));
+  return sync_and_check(h);
+}
+
+static int finite_all(const double *v, int n) {
+  for (int i = 0; i < n; i++)
+    if (!isfinite(v[i])) return 0;
+  return 1;
+}
+
+int he4_step_rk(he4_handle *hh, double deltat, double means[9]) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  if (!isfinite(deltat)) {
+    set_error("deltat is not finite");
+    return HE4_E_ARG;
+  }
+  HE4_TRY(step_rk(h, deltat, h->scal));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (means) memcpy(means, h->hscal + 3, 9 * sizeof(double));
+  if (!finite_all(h->hscal, 12)) {
+    set_error("non-finite trajectory means after steprk");
+    return HE4_E_NONFINITE;
+  }
+  return HE4_OK;
+}
+
+int he4_step_pc(he4_handle *hh, double deltat, double err[3], double means[9]) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  if (!isfinite(deltat)) {
+    set_error("deltat is not finite");
+    return HE4_E_ARG;
+  }
+  HE4_TRY(step_pc(h, deltat, h->scal));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (err) memcpy(err, h->hscal, 3 * sizeof(double));
+  if (means) memcpy(means, h->hscal + 3, 9 * sizeof(double));
+  if (!finite_all(h->hscal, 12)) {
+    set_error("non-finite errHe/errimp/errvimp or means after steppc");
+    return HE4_E_NONFINITE;
+  }
+  return HE4_OK;
+}
+
+int he4_run(he4_handle *hh, int32_t nsteps, double deltat, double *err, double *means) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  if (nsteps < 0 || !isfinite(deltat)) {
+    set_error("invalid nsteps or deltat");
+    return HE4_E_ARG;
+  }
+  if (nsteps == 0) return HE4_OK;
+  double *dres = nullptr;
+  HE4_CUDA_TRY(cudaMallocAsync((void **)&dres, sizeof(double) * 12 * nsteps, h->stream));
+  int e = HE4_OK;
+  for (int s = 0; s < nsteps && e == HE4_OK; s++) {
+    if (h->nsteps_done < 3)
+      e = step_rk(h, deltat, dres + 12 * s);
+    else
+      e = step_pc(h, deltat, dres + 12 * s);
+  }
+  double *hres = nullptr;
+  if (e == HE4_OK) {
+    hres = (double *)malloc(sizeof(double) * 12 * nsteps);
+    cudaError_t ce = cudaMemcpyAsync(hres, dres, sizeof(double) * 12 * nsteps, cudaMemcpyDeviceToHost, h->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+    if (ce != cudaSuccess) {
+      set_error("he4_run copy-out: %s", cudaGetErrorString(ce));
+      e = HE4_E_CUDA;
+    }
+  }
+  cudaFreeAsync(dres, h->stream);
+  if (e == HE4_OK) {
+    for (int s = 0; s < nsteps; s++) {
+      if (err) memcpy(err + 3 * s, hres + 12 * s, 3 * sizeof(double));
+      if (means) memcpy(means + 9 * s, hres + 12 * s + 3, 9 * sizeof(double));
+    }
+    if (!finite_all(hres, 12 * nsteps)) {
+      set_error("non-finite errors or means during he4_run");
+      e = HE4_E_NONFINITE;
+    }
+  }
+  free(hres);
+  return e;
+}
+
+int he4_energy(he4_handle *hh, he4_energies *e) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  if (!e) {
+    set_error("null energies");
+    return HE4_E_ARG;
+  }
+  HE4_TRY(compute_energy(h, e));
+  const double *v = &e->etot;
+  if (!finite_all(v, 11)) {
+    set_error("non-finite energy");
+    return HE4_E_NONFINITE;
+  }
+  return HE4_OK;
+}
+
+int he4_get_field(he4_handle *hh, int32_t which, double *out) {
+  HANDLE_OR_FAIL(hh);
+  if (!out) {
+    set_error("null output");
+    return HE4_E_ARG;
+  }
+  const double *src = nullptr;
+  switch (which) {
+    case HE4_F_DEN: src = h->den; break;
+    case HE4_F_POT4: src = h->pot4; break;
+    case HE4_F_DENX: src = h->denx; break;
+    case HE4_F_PSIX: src = h->psix; break;
+    case HE4_F_HPSIX: src = h->hpsix; break;
+    case HE4_F_UIMP: src = h->uimp; break;
+    case HE4_F_DENCG: src = h->dencg; break;
+    case HE4_F_DELJ4: src = h->delj4; break;
+    case HE4_F_DENALF: src = h->denalf; break;
+    case HE4_F_UALPHAS: src = h->ualphas; break;
+    case HE4_F_FALFS: src = h->falfs; break;
+    case HE4_F_INTXALF: src = h->intx; break;
+    case HE4_F_INTYALF: src = h->inty; break;
+    case HE4_F_INTZALF: src = h->intz; break;
+    case HE4_F_DXDEN: src = h->dxden; break;
+    case HE4_F_DYDEN: src = h->dyden; break;
+    case HE4_F_DZDEN: src = h->dzden; break;
+    case HE4_F_FX: src = h->fx; break;
+    case HE4_F_FY: src = h->fy; break;
+    case HE4_F_FZ: src = h->fz; break;
+    case HE4_F_PENALTY: src = h->penalty; break;
+    case HE4_F_CORR: src = h->corr; break;
+    default:
+      set_error("unknown field id %d", which);
+      return HE4_E_ARG;
+  }
+  HE4_CUDA_TRY(cudaMemcpyAsync(out, src, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+int he4_get_kernel(he4_handle *hh, int32_t which, double *out) {
+  HANDLE_OR_FAIL(hh);
+  if (!out) {
+    set_error("null output");
+    return HE4_E_ARG;
+  }
+  const double *src = nullptr;
+  switch (which) {
+    case HE4_K_WCGK: src = h->wcgk; break;
+    case HE4_K_FVLJ4: src = h->fvlj4; break;
+    case HE4_K_KALFS: src = h->kalfs; break;
+    case HE4_K_VQ: src = h->vq; break;
+    case HE4_K_PMOD: src = h->pmod; break;
+    default:
+      set_error("unknown kernel id %d", which);
+      return HE4_E_ARG;
+  }
+  HE4_CUDA_TRY(cudaMemcpyAsync(out, src, sizeof(double) * h->H, cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+int he4_fft_r2c(he4_handle *hh, const double *in, double *out) {
+  HANDLE_OR_FAIL(hh);
+  if (!in || !out) {
+    set_error("null buffer");
+    return HE4_E_ARG;
+  }
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->rtmp[0], in, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+  const double *src[1] = {h->rtmp[0]};
+  double2 *dst[1] = {h->spec[4] ? h->spec[4] : h->spec[1]};
+  HE4_TRY(fft_r2c(h, 1, src, dst));
+  HE4_TRY(fft_z_only(h, dst[0], false));
+  HE4_CUDA_TRY(cudaMemcpyAsync(out, dst[0], sizeof(double2) * h->H, cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+int he4_fft_c2r(he4_handle *hh, const double *in, double *out) {
+  HANDLE_OR_FAIL(hh);
+  if (!in || !out) {
+    set_error("null buffer");
+    return HE4_E_ARG;
+  }
+  double2 *buf = h->spec[4] ? h->spec[4] : h->spec[1];
+  HE4_CUDA_TRY(cudaMemcpyAsync(buf, in, sizeof(double2) * h->H, cudaMemcpyHostToDevice, h->stream));
+  HE4_TRY(fft_z_only(h, buf, true));
+  double2 *src[1] = {buf};
+  double *dst[1] = {h->rtmp[0]};
+  HE4_TRY(fft_c2r(h, 1, src, dst));
+  HE4_CUDA_TRY(cudaMemcpyAsync(out, h->rtmp[0], sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+static int launch_bench(Handle *h, int which) {
+  switch (which) {
+    case 0: {
+      ZOp op{h->spec[0], h->spec[1], h->wcgk, h->renor, -1};
+      return fft_z_conv(h, 1, &op);
+    }
+    case 1: {
+      double2 *b[1] = {h->spec[1]};
+      return fft_y(h, 1, b, false);
+    }
+    case 2: return fft_x_only(h, h->rtmp[0], h->spec[1], nullptr, nullptr, false);
+    case 3: return fft_x_only(h, nullptr, nullptr, h->spec[1], h->rtmp[0], true);
+    default: set_error("unknown kernel id %d", which); return HE4_E_ARG;
+  }
+}
+
+int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per_launch, double *bytes_per_launch,
+                     char *name, int32_t name_len) {
+  HANDLE_OR_FAIL(hh);
+  if (reps < 1 || !ms_per_launch || !bytes_per_launch) {
+    set_error("invalid arguments");
+    return HE4_E_ARG;
+  }
+  static const char *names[4] = {"k_fft_z_conv", "k_fft_y", "k_fft_x_r2c", "k_fft_x_c2r"};
+  const double H = (double)h->H, N = (double)h->N;
+  // algorithmic bytes: read input once, write output once (+ the real kernel)
+  const double bytes[4] = {16 * H + 8 * H + 16 * H, 2 * 16 * H, 8 * N + 16 * H, 16 * H + 8 * N};
+  if (which < 0 || which > 3) {
+    set_error("unknown kernel id %d", which);
+    return HE4_E_ARG;
+  }
+  HE4_TRY(launch_bench(h, which));  // warm-up
+  cudaEvent_t e0, e1;
+  HE4_CUDA_TRY(cudaEventCreate(&e0));
+  HE4_CUDA_TRY(cudaEventCreate(&e1));
+  HE4_CUDA_TRY(cudaEventRecord(e0, h->stream));
+  int rc = HE4_OK;
+  for (int i = 0; i < reps && rc == HE4_OK; i++) rc = launch_bench(h, which);
+  HE4_CUDA_TRY(cudaEventRecord(e1, h->stream));
+  HE4_CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  HE4_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  HE4_TRY(rc);
+  *ms_per_launch = ms / reps;
+  *bytes_per_launch = bytes[which];
+  if (name && name_len > 0) {
+    strncpy(name, names[which], name_len - 1);
+    name[name_len - 1] = 0;
+  }
+  return HE4_OK;
+}
+
+int he4_get_stream(he4_handle *hh, void **stream) {
+  HANDLE_OR_FAIL(hh);
+  if (!stream) return HE4_E_ARG;
+  *stream = (void *)h->stream;
+  return HE4_OK;
+}
+
+int64_t he4_launch_count(he4_handle *hh) { return hh ? hh->h.launches : -1; }
+
+const char *he4_strerror(int code) {
+  switch (code) {
+    case HE4_OK: return "ok";
+    case HE4_E_ARG: return "invalid argument";
+    case HE4_E_UNSUPPORTED: return "unsupported configuration";
+    case HE4_E_NOMEM: return "out of memory";
+    case HE4_E_CUDA: return "CUDA error";
+    case HE4_E_STATE: return "invalid call order";
+    case HE4_E_NONFINITE: return "non-finite result";
+    case HE4_E_NODEVICE: return "no sm_100 device";
+    default: return "unknown error";
+  }
+}
+
+const char *he4_last_error(void) { return g_err; }
+
+}  // extern "C"

@@ -1,0 +1,181 @@
+// common.cuh -- shared declarations of the B200 time-step library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+
+#include "../../include/he4_tddft.h"
+
+namespace he4 {
+
+// ---------------------------------------------------------------------------
+// error handling: every failing call records a message and returns a code.
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+
+#define HE4_CUDA_TRY(expr)                                                      \
+  do {                                                                          \
+    cudaError_t e_ = (expr);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      ::he4::set_error("%s:%d %s: %s", __FILE__, __LINE__, #expr,               \
+                       cudaGetErrorString(e_));                                 \
+      return HE4_E_CUDA;                                                        \
+    }                                                                           \
+  } while (0)
+
+#define HE4_TRY(expr)            \
+  do {                           \
+    int r_ = (expr);             \
+    if (r_ != HE4_OK) return r_; \
+  } while (0)
+
+// after a kernel launch: record launch and check the launch error
+#define HE4_LAUNCHED(h)                                                          \
+  do {                                                                           \
+    (h)->launches++;                                                             \
+    cudaError_t e_ = cudaGetLastError();                                         \
+    if (e_ != cudaSuccess) {                                                     \
+      ::he4::set_error("%s:%d kernel launch: %s", __FILE__, __LINE__,            \
+                       cudaGetErrorString(e_));                                  \
+      return HE4_E_CUDA;                                                         \
+    }                                                                            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// complex FP64 helpers
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ double2 cmk(double a, double b) { return make_double2(a, b); }
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__host__ __device__ __forceinline__ double2 cmuli(double2 a) {
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// ---------------------------------------------------------------------------
+// FFT plan
+// ---------------------------------------------------------------------------
+constexpr int kMaxStages = 12;
+struct AxisPlan {
+  int n = 0;
+  int nst = 0;
+  int radix[kMaxStages] = {0};
+  double2 *tw = nullptr;  // device: exp(-2 pi i t / n), t in [0, n)
+};
+
+struct FftPlan {
+  int nx = 0, ny = 0, nz = 0, nxh = 0;
+  AxisPlan ax, ay, az;
+  int wy = 8, wz = 8;   // pencils per CTA in the y and z passes
+  int px = 8;           // complex pencils (= row pairs) per CTA in the x pass
+};
+
+int fft_plan_init(FftPlan &P, int nx, int ny, int nz);
+void fft_plan_free(FftPlan &P);
+
+// ---------------------------------------------------------------------------
+// stencil weights (centre row of the Bickley matrix, times 1/h^order)
+// ---------------------------------------------------------------------------
+struct Stencil {
+  int m = 3;                 // half width, npd = 2m+1
+  double w1[3][25];          // first derivative, per axis
+  double w2[3][25];          // second derivative, per axis
+};
+int fd_weights(int npd, int order, double *w);
+
+struct ZOp;  // z-pass operation (fft.cu)
+
+// ---------------------------------------------------------------------------
+// the handle
+// ---------------------------------------------------------------------------
+struct Handle {
+  he4_params p{};
+  int nx = 0, ny = 0, nz = 0, nxh = 0, npar = 0;
+  size_t N = 0, H = 0;
+  double hx = 0, hy = 0, hz = 0, dxyz = 0, renor = 0, mAg_u = 0, h2o2mx = 0;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+  FftPlan fft;
+  Stencil st;
+
+  // k-space kernels [H] and derivative symbols
+  double *wcgk = nullptr, *fvlj4 = nullptr, *kalfs = nullptr, *vq = nullptr, *pmod = nullptr;
+  double *dsym = nullptr;     // [nx+ny+nz]: imaginary part of the periodic first-derivative symbol
+  double *timec_re = nullptr; // [nz]
+
+  // He fields
+  double2 *psi = nullptr, *psiold[3] = {nullptr, nullptr, nullptr}, *hpsiold[2] = {nullptr, nullptr};
+  double2 *pc = nullptr, *q = nullptr, *ctmp = nullptr;
+  double *den = nullptr, *pot4 = nullptr, *dencg = nullptr, *delj4 = nullptr, *denalf = nullptr;
+  double *ualphas = nullptr, *falfs = nullptr, *intx = nullptr, *inty = nullptr, *intz = nullptr;
+  double *dxden = nullptr, *dyden = nullptr, *dzden = nullptr, *penalty = nullptr, *corr = nullptr;
+  double *denx = nullptr, *psix = nullptr, *hpsix = nullptr, *uimp = nullptr;
+  double *fx = nullptr, *fy = nullptr, *fz = nullptr;
+  double *rtmp[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned int *counts = nullptr;
+  // spectra work buffers [H] complex
+  double2 *spec[8] = {nullptr};
+
+  // particles [3][npar]
+  double *rimp = nullptr, *vimp = nullptr, *aimp = nullptr;
+  double *rimpold[3] = {nullptr}, *vimpold[3] = {nullptr}, *aimpold[2] = {nullptr};
+  double *qr = nullptr, *qv = nullptr, *pcr = nullptr, *pcv = nullptr;
+  int ioldp[3] = {0, 1, 2}, ioldh[2] = {0, 1}, ioldr[3] = {0, 1, 2}, ioldv[3] = {0, 1, 2}, iolda[2] = {0, 1};
+
+  // reductions
+  double *red = nullptr;      // partial sums workspace
+  double *scal = nullptr;     // device scalars (errors, energies, means)
+  double *hscal = nullptr;    // pinned host mirror of scal
+
+  int have_state = 0;
+  int nsteps_done = 0;
+  size_t red_len = 0;
+};
+
+// kernel-level entry points used by the ABI layer
+int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out);
+int fft_c2r(Handle *h, int n, double2 *const *in, double *const *out);
+int fft_y(Handle *h, int n, double2 *const *buf, bool inverse);
+// z pass: for each op, out = IFFT_z(coef * K * FFT_z(in)); K may be null (=1)
+// or the derivative symbol of an axis (kind 1..3).
+struct ZOp {
+  const double2 *in;
+  double2 *out;
+  const double *kern;
+  double coef;
+  int dsym_axis;  // -1 none, 0/1/2: multiply by i*dsym[axis](k)
+  int mode = 0;   // 0: FFT_z, multiply, IFFT_z; 1: FFT_z only; 2: IFFT_z only
+};
+int fft_z_conv(Handle *h, int n, const ZOp *ops);
+// plain transform along z of one half spectrum, in place
+int fft_z_only(Handle *h, double2 *buf, bool inverse);
+// x pass alone (R2C: rin -> cout; C2R: cin -> rout)
+int fft_x_only(Handle *h, const double *rin, double2 *cout, const double2 *cin, double *rout, bool inverse);
+
+int setup_kernels(Handle *h);
+
+int field_potenimp(Handle *h);
+int field_poten(Handle *h);
+int field_forceimp(Handle *h);
+
+// dres: device array of 12 doubles: errHe, errimp, errvimp, then the 9 means
+int step_rk(Handle *h, double dt, double *dres);
+int step_pc(Handle *h, double dt, double *dres);
+int compute_energy(Handle *h, he4_energies *e);
+int compute_den(Handle *h);
+int particle_means(Handle *h, double *means);
+
+}  // namespace he4
+
+struct he4_handle {
+  he4::Handle h;
+};

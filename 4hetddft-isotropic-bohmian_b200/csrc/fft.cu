@@ -1,0 +1,540 @@
+// fft.cu -- batched 3D real FFTs for the convolutions of the mean field.
+//
+// Replaces the FFTW plans and their executions (fft.f90:43-65, 79-207).
+// Layout: real grids [nz][ny][nx]; half spectra [nz][ny][nx/2+1] (the FFTW
+// r2c layout of the reference).  Forward transforms are unnormalised; the
+// reference's backward scaling by renor = 1/N (fft.f90:130,138,...) is folded
+// into the coefficient of the k-space multiply of the z pass.
+//
+// A 3D transform is three passes over HBM:
+//   x pass  (R2C / C2R): two real rows packed into one complex pencil,
+//   y pass  (complex), and
+//   z pass  (complex) fused with the k-space kernel multiply and the inverse
+//           z transform: FFT_z -> coef*K(k) (*i*D(k)) -> IFFT_z in one launch.
+// Each CTA stages a tile of pencils in shared memory and runs a mixed-radix
+// (2/3/4/5) Stockham transform between two shared buffers; pencils of one
+// tile are contiguous in x so every global access is a coalesced segment.
+#include <math.h>
+#include <stdlib.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace he4 {
+
+static constexpr double kC3S = 0.86602540378443864676372317075293618;   // sin(2pi/3)
+static constexpr double kC5C1 = 0.30901699437494742410229341718281906;  // cos(2pi/5)
+static constexpr double kC5C2 = -0.80901699437494742410229341718281906; // cos(4pi/5)
+static constexpr double kC5S1 = 0.95105651629515357211643933337938214;  // sin(2pi/5)
+static constexpr double kC5S2 = 0.58778525229247312916870595463907277;  // sin(4pi/5)
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// small DFTs (forward: exp(-2 pi i jk/R); inverse: conjugate roots)
+// ---------------------------------------------------------------------------
+template <int R, bool INV>
+struct Dft;
+
+template <bool INV>
+struct Dft<2, INV> {
+  static __device__ __forceinline__ void run(double2 *u) {
+    double2 t = u[0];
+    u[0] = cadd(t, u[1]);
+    u[1] = csub(t, u[1]);
+  }
+};
+
+template <bool INV>
+struct Dft<4, INV> {
+  static __device__ __forceinline__ void run(double2 *u) {
+    double2 a = cadd(u[0], u[2]), b = csub(u[0], u[2]);
+    double2 c = cadd(u[1], u[3]), d = cmuli<INV>(csub(u[1], u[3]));
+    u[0] = cadd(a, c);
+    u[2] = csub(a, c);
+    u[1] = cadd(b, d);
+    u[3] = csub(b, d);
+  }
+};
+
+template <bool INV>
+struct Dft<3, INV> {
+  static __device__ __forceinline__ void run(double2 *u) {
+    double2 t1 = cadd(u[1], u[2]);
+    double2 t2 = csub(u[0], cscale(t1, 0.5));
+    double2 t3 = cscale(cmuli<INV>(csub(u[1], u[2])), kC3S);
+    u[0] = cadd(u[0], t1);
+    u[1] = cadd(t2, t3);
+    u[2] = csub(t2, t3);
+  }
+};
+
+template <bool INV>
+struct Dft<5, INV> {
+  static __device__ __forceinline__ void run(double2 *u) {
+    double2 a1 = cadd(u[1], u[4]), b1 = csub(u[1], u[4]);
+    double2 a2 = cadd(u[2], u[3]), b2 = csub(u[2], u[3]);
+    double2 r1 = cadd(u[0], cadd(cscale(a1, kC5C1), cscale(a2, kC5C2)));
+    double2 r2 = cadd(u[0], cadd(cscale(a1, kC5C2), cscale(a2, kC5C1)));
+    double2 s1 = cmuli<INV>(cadd(cscale(b1, kC5S1), cscale(b2, kC5S2)));
+    double2 s2 = cmuli<INV>(csub(cscale(b1, kC5S2), cscale(b2, kC5S1)));
+    u[0] = cadd(u[0], cadd(a1, a2));
+    u[1] = cadd(r1, s1);
+    u[4] = csub(r1, s1);
+    u[2] = cadd(r2, s2);
+    u[3] = csub(r2, s2);
+  }
+};
+
+// One Stockham stage on W pencils stored [n][ld] (pencil w at column w):
+// butterfly i of pencil w reads x[i + j n/R], applies w_{pR}^{jk}
+// (k = i mod p), runs the R-point DFT and writes y[(i/p) p R + k + j p].
+template <int R, bool INV>
+__device__ __forceinline__ void stage(const double2 *__restrict__ src, double2 *__restrict__ dst, int n,
+                                      int p, int W, int ld, const double2 *__restrict__ tw) {
+  const int m = n / R, tstep = n / (p * R);
+  const int nb = m * W;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    const int w = b % W, i = b / W, k = i % p;
+    double2 u[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) u[j] = src[(i + j * m) * ld + w];
+    if (k) {
+#pragma unroll
+      for (int j = 1; j < R; j++) {
+        double2 t = tw[j * k * tstep];
+        if (INV) t.y = -t.y;
+        u[j] = cmul(u[j], t);
+      }
+    }
+    Dft<R, INV>::run(u);
+    const int j0 = (i / p) * p * R + k;
+#pragma unroll
+    for (int j = 0; j < R; j++) dst[(j0 + j * p) * ld + w] = u[j];
+  }
+}
+
+// Full transform of W pencils; a holds the input, b is scratch.  Returns the
+// buffer holding the natural-order result.
+template <bool INV>
+__device__ double2 *fft_smem(double2 *a, double2 *b, const AxisPlan &P, int W, int ld,
+                             const double2 *__restrict__ tw) {
+  int p = 1;
+  for (int s = 0; s < P.nst; s++) {
+    const int R = P.radix[s];
+    switch (R) {
+      case 4: stage<4, INV>(a, b, P.n, p, W, ld, tw); break;
+      case 2: stage<2, INV>(a, b, P.n, p, W, ld, tw); break;
+      case 3: stage<3, INV>(a, b, P.n, p, W, ld, tw); break;
+      default: stage<5, INV>(a, b, P.n, p, W, ld, tw); break;
+    }
+    __syncthreads();
+    double2 *t = a;
+    a = b;
+    b = t;
+    p *= R;
+  }
+  return a;
+}
+
+__device__ __forceinline__ void load_tw(double2 *s_tw, const AxisPlan &P) {
+  for (int t = threadIdx.x; t < P.n; t += blockDim.x) s_tw[t] = P.tw[t];
+}
+
+// ---------------------------------------------------------------------------
+// x pass
+// ---------------------------------------------------------------------------
+constexpr int kMaxBatch = 8;
+
+struct XArgs {
+  AxisPlan ax;
+  int nxh, P;
+  long nrow;
+  double scale;
+  const double *rin[kMaxBatch];
+  double2 *cout[kMaxBatch];
+  const double2 *cin[kMaxBatch];
+  double *rout[kMaxBatch];
+};
+
+__global__ void __launch_bounds__(kThreads) k_fft_x_r2c(XArgs a) {
+  extern __shared__ double2 smem[];
+  const int n = a.ax.n, P = a.P, ld = P + 1, nxh = a.nxh;
+  double2 *b0 = smem, *b1 = smem + n * ld, *tw = smem + 2 * n * ld;
+  load_tw(tw, a.ax);
+  const double *in = a.rin[blockIdx.y];
+  double2 *out = a.cout[blockIdx.y];
+  const long row0 = (long)blockIdx.x * 2 * P;
+  for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+    const int q = e / n, x = e - q * n;
+    const long ra = row0 + 2 * q, rb = ra + 1;
+    double va = (ra < a.nrow) ? in[ra * n + x] : 0.0;
+    double vb = (rb < a.nrow) ? in[rb * n + x] : 0.0;
+    b0[x * ld + q] = make_double2(va, vb);
+  }
+  __syncthreads();
+  double2 *res = fft_smem<false>(b0, b1, a.ax, P, ld, tw);
+  for (int e = threadIdx.x; e < nxh * P; e += blockDim.x) {
+    const int q = e / nxh, k = e - q * nxh;
+    const long ra = row0 + 2 * q, rb = ra + 1;
+    const double2 zk = res[k * ld + q];
+    const double2 zm = cconj(res[((n - k) % n) * ld + q]);
+    const double2 A = cscale(cadd(zk, zm), 0.5);
+    const double2 d = cscale(csub(zk, zm), 0.5);
+    if (ra < a.nrow) out[ra * nxh + k] = A;
+    if (rb < a.nrow) out[rb * nxh + k] = make_double2(d.y, -d.x);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_fft_x_c2r(XArgs a) {
+  extern __shared__ double2 smem[];
+  const int n = a.ax.n, P = a.P, ld = P + 1, nxh = a.nxh;
+  double2 *b0 = smem, *b1 = smem + n * ld, *tw = smem + 2 * n * ld;
+  load_tw(tw, a.ax);
+  const double2 *in = a.cin[blockIdx.y];
+  double *out = a.rout[blockIdx.y];
+  const long row0 = (long)blockIdx.x * 2 * P;
+  for (int e = threadIdx.x; e < nxh * P; e += blockDim.x) {
+    const int q = e / nxh, k = e - q * nxh;
+    const long ra = row0 + 2 * q, rb = ra + 1;
+    double2 X = (ra < a.nrow) ? in[ra * nxh + k] : make_double2(0.0, 0.0);
+    double2 Y = (rb < a.nrow) ? in[rb * nxh + k] : make_double2(0.0, 0.0);
+    if (k == 0 || 2 * k == n) {  // DC / Nyquist of a real transform: drop Im
+      X.y = 0.0;
+      Y.y = 0.0;
+    }
+    b0[k * ld + q] = make_double2(X.x - Y.y, X.y + Y.x);  // X + iY
+    if (k > 0 && n - k >= nxh) b0[(n - k) * ld + q] = make_double2(X.x + Y.y, Y.x - X.y);  // conj(X) + i conj(Y)
+  }
+  __syncthreads();
+  double2 *res = fft_smem<true>(b0, b1, a.ax, P, ld, tw);
+  const double sc = a.scale;
+  for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+    const int q = e / n, x = e - q * n;
+    const long ra = row0 + 2 * q, rb = ra + 1;
+    const double2 v = res[x * ld + q];
+    if (ra < a.nrow) out[ra * n + x] = v.x * sc;
+    if (rb < a.nrow) out[rb * n + x] = v.y * sc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pencil enumeration for the y and z passes over a half spectrum
+// [nz][ny][nxh].  Pencils are (kx, o) pairs, o = z for the y pass and o = y
+// for the z pass.  Tiles of W pencils with consecutive kx come first; the
+// nxh mod W leftover columns are grouped across o in the last tiles.
+// ---------------------------------------------------------------------------
+struct PencilMap {
+  int nxh, nother, W;
+  long so;  // stride between consecutive o
+};
+
+__device__ __forceinline__ long pencil_offset(const PencilMap &m, long pid, int *kx_out, int *o_out) {
+  const int nfull = m.nxh / m.W;
+  const long main = (long)nfull * m.W * m.nother;
+  const long total = (long)m.nxh * m.nother;
+  if (pid >= total) return -1;
+  int kx, o;
+  if (pid < main) {
+    const long per = (long)nfull * m.W;
+    o = (int)(pid / per);
+    kx = (int)(pid - (long)o * per);
+  } else {
+    const int tw = m.nxh - nfull * m.W;
+    const long r = pid - main;
+    o = (int)(r / tw);
+    kx = nfull * m.W + (int)(r - (long)o * tw);
+  }
+  *kx_out = kx;
+  *o_out = o;
+  return (long)o * m.so + kx;
+}
+
+struct YArgs {
+  AxisPlan ay;
+  PencilMap map;
+  long sf;  // element stride along the transformed axis
+  double2 *buf[kMaxBatch];
+};
+
+template <bool INV>
+__global__ void __launch_bounds__(kThreads) k_fft_y(YArgs a) {
+  extern __shared__ double2 smem[];
+  const int n = a.ay.n, W = a.map.W;
+  double2 *b0 = smem, *b1 = smem + n * W, *tw = smem + 2 * n * W;
+  long *offs = reinterpret_cast<long *>(tw + n);
+  load_tw(tw, a.ay);
+  for (int w = threadIdx.x; w < W; w += blockDim.x) {
+    int kx, o;
+    offs[w] = pencil_offset(a.map, (long)blockIdx.x * W + w, &kx, &o);
+  }
+  __syncthreads();
+  double2 *data = a.buf[blockIdx.y];
+  for (int e = threadIdx.x; e < n * W; e += blockDim.x) {
+    const int w = e % W, j = e / W;
+    const long off = offs[w];
+    b0[j * W + w] = (off >= 0) ? data[off + j * a.sf] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  double2 *res = fft_smem<INV>(b0, b1, a.ay, W, W, tw);
+  for (int e = threadIdx.x; e < n * W; e += blockDim.x) {
+    const int w = e % W, j = e / W;
+    const long off = offs[w];
+    if (off >= 0) data[off + j * a.sf] = res[j * W + w];
+  }
+}
+
+struct ZArgs {
+  AxisPlan az;
+  PencilMap map;
+  long sf;
+  int nx, ny, nz;
+  const double *dsym;  // [nx | ny | nz]
+  ZOp ops[kMaxBatch];
+};
+
+__global__ void __launch_bounds__(kThreads) k_fft_z_conv(ZArgs a) {
+  extern __shared__ double2 smem[];
+  const int n = a.az.n, W = a.map.W;
+  double2 *b0 = smem, *b1 = smem + n * W, *tw = smem + 2 * n * W;
+  long *offs = reinterpret_cast<long *>(tw + n);
+  int *kxs = reinterpret_cast<int *>(offs + W);
+  int *kys = kxs + W;
+  load_tw(tw, a.az);
+  for (int w = threadIdx.x; w < W; w += blockDim.x) {
+    int kx = 0, o = 0;
+    offs[w] = pencil_offset(a.map, (long)blockIdx.y * W + w, &kx, &o);
+    kxs[w] = kx;
+    kys[w] = o;
+  }
+  __syncthreads();
+  const ZOp op = a.ops[blockIdx.x];
+  for (int e = threadIdx.x; e < n * W; e += blockDim.x) {
+    const int w = e % W, j = e / W;
+    const long off = offs[w];
+    b0[j * W + w] = (off >= 0) ? op.in[off + j * a.sf] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  if (op.mode != 0) {  // plain forward or inverse transform along z
+    double2 *r = (op.mode == 1) ? fft_smem<false>(b0, b1, a.az, W, W, tw) : fft_smem<true>(b0, b1, a.az, W, W, tw);
+    for (int e = threadIdx.x; e < n * W; e += blockDim.x) {
+      const int w = e % W, j = e / W;
+      const long off = offs[w];
+      if (off >= 0) op.out[off + j * a.sf] = r[j * W + w];
+    }
+    return;
+  }
+  double2 *res = fft_smem<false>(b0, b1, a.az, W, W, tw);
+  double2 *wk = (res == b0) ? b1 : b0;
+  for (int e = threadIdx.x; e < n * W; e += blockDim.x) {
+    const int w = e % W, j = e / W;
+    const long off = offs[w];
+    double c = op.coef;
+    if (off >= 0 && op.kern) c *= op.kern[off + j * a.sf];
+    double2 v = cscale(res[j * W + w], c);
+    if (op.dsym_axis >= 0) {
+      double ds;
+      if (op.dsym_axis == 0) ds = a.dsym[kxs[w]];
+      else if (op.dsym_axis == 1) ds = a.dsym[a.nx + kys[w]];
+      else ds = a.dsym[a.nx + a.ny + j];
+      v = make_double2(-v.y * ds, v.x * ds);  // times i*ds
+    }
+    wk[j * W + w] = v;
+  }
+  __syncthreads();
+  double2 *out = (wk == b0) ? fft_smem<true>(b0, b1, a.az, W, W, tw) : fft_smem<true>(b1, b0, a.az, W, W, tw);
+  for (int e = threadIdx.x; e < n * W; e += blockDim.x) {
+    const int w = e % W, j = e / W;
+    const long off = offs[w];
+    if (off >= 0) op.out[off + j * a.sf] = out[j * W + w];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static int axis_init(AxisPlan &A, int n) {
+  A.n = n;
+  A.nst = 0;
+  int r = n;
+  while (r % 4 == 0) { A.radix[A.nst++] = 4; r /= 4; }
+  while (r % 2 == 0) { A.radix[A.nst++] = 2; r /= 2; }
+  while (r % 3 == 0) { A.radix[A.nst++] = 3; r /= 3; }
+  while (r % 5 == 0) { A.radix[A.nst++] = 5; r /= 5; }
+  if (r != 1 || A.nst > kMaxStages) {
+    set_error("FFT length %d is not of the form 2^a 3^b 5^c", n);
+    return HE4_E_UNSUPPORTED;
+  }
+  double2 *tw = (double2 *)malloc(sizeof(double2) * n);
+  for (int t = 0; t < n; t++) {
+    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
+    tw[t] = make_double2((double)cosl(ang), (double)sinl(ang));
+  }
+  cudaError_t e = cudaMalloc(&A.tw, sizeof(double2) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(A.tw, tw, sizeof(double2) * n, cudaMemcpyHostToDevice);
+  free(tw);
+  if (e != cudaSuccess) {
+    set_error("twiddle upload: %s", cudaGetErrorString(e));
+    return HE4_E_CUDA;
+  }
+  return HE4_OK;
+}
+
+static int tile_width(int n) {
+  int w = 2048 / n;
+  w = (w / 8) * 8;
+  return std::max(8, std::min(32, w));
+}
+
+static size_t smem_x(const FftPlan &P) { return sizeof(double2) * (2 * (size_t)P.nx * (P.px + 1) + P.nx); }
+static size_t smem_yz(int n, int W) {
+  return sizeof(double2) * (2 * (size_t)n * W + n) + sizeof(long) * W + 2 * sizeof(int) * W;
+}
+
+int fft_plan_init(FftPlan &P, int nx, int ny, int nz) {
+  P.nx = nx;
+  P.ny = ny;
+  P.nz = nz;
+  P.nxh = nx / 2 + 1;
+  HE4_TRY(axis_init(P.ax, nx));
+  HE4_TRY(axis_init(P.ay, ny));
+  HE4_TRY(axis_init(P.az, nz));
+  P.px = tile_width(nx);
+  P.wy = tile_width(ny);
+  P.wz = tile_width(nz);
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x(P)));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x(P)));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(ny, P.wy)));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(ny, P.wy)));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(nz, P.wz)));
+  return HE4_OK;
+}
+
+void fft_plan_free(FftPlan &P) {
+  cudaFree(P.ax.tw);
+  cudaFree(P.ay.tw);
+  cudaFree(P.az.tw);
+  P.ax.tw = P.ay.tw = P.az.tw = nullptr;
+}
+
+int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out) {
+  const FftPlan &P = h->fft;
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    int nb = std::min(kMaxBatch, n - b0);
+    XArgs a{};
+    a.ax = P.ax;
+    a.nxh = P.nxh;
+    a.P = P.px;
+    a.nrow = (long)P.ny * P.nz;
+    a.scale = 1.0;
+    for (int i = 0; i < nb; i++) {
+      a.rin[i] = in[b0 + i];
+      a.cout[i] = out[b0 + i];
+    }
+    dim3 grid((unsigned)((a.nrow + 2 * P.px - 1) / (2 * P.px)), nb);
+    k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+    HE4_LAUNCHED(h);
+  }
+  double2 *bufs[64];
+  for (int i = 0; i < n; i++) bufs[i] = out[i];
+  HE4_TRY(fft_y(h, n, bufs, false));
+  return HE4_OK;
+}
+
+int fft_y(Handle *h, int n, double2 *const *buf, bool inverse) {
+  const FftPlan &P = h->fft;
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    int nb = std::min(kMaxBatch, n - b0);
+    YArgs a{};
+    a.ay = P.ay;
+    a.map.nxh = P.nxh;
+    a.map.nother = P.nz;
+    a.map.W = P.wy;
+    a.map.so = (long)P.ny * P.nxh;
+    a.sf = P.nxh;
+    for (int i = 0; i < nb; i++) a.buf[i] = buf[b0 + i];
+    long total = (long)P.nxh * P.nz;
+    dim3 grid((unsigned)((total + P.wy - 1) / P.wy), nb);
+    if (inverse)
+      k_fft_y<true><<<grid, kThreads, smem_yz(P.ny, P.wy), h->stream>>>(a);
+    else
+      k_fft_y<false><<<grid, kThreads, smem_yz(P.ny, P.wy), h->stream>>>(a);
+    HE4_LAUNCHED(h);
+  }
+  return HE4_OK;
+}
+
+int fft_c2r(Handle *h, int n, double2 *const *in, double *const *out) {
+  const FftPlan &P = h->fft;
+  HE4_TRY(fft_y(h, n, in, true));
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    int nb = std::min(kMaxBatch, n - b0);
+    XArgs a{};
+    a.ax = P.ax;
+    a.nxh = P.nxh;
+    a.P = P.px;
+    a.nrow = (long)P.ny * P.nz;
+    a.scale = 1.0;
+    for (int i = 0; i < nb; i++) {
+      a.cin[i] = in[b0 + i];
+      a.rout[i] = out[b0 + i];
+    }
+    dim3 grid((unsigned)((a.nrow + 2 * P.px - 1) / (2 * P.px)), nb);
+    k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+    HE4_LAUNCHED(h);
+  }
+  return HE4_OK;
+}
+
+int fft_z_conv(Handle *h, int n, const ZOp *ops) {
+  const FftPlan &P = h->fft;
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    int nb = std::min(kMaxBatch, n - b0);
+    ZArgs a{};
+    a.az = P.az;
+    a.map.nxh = P.nxh;
+    a.map.nother = P.ny;
+    a.map.W = P.wz;
+    a.map.so = P.nxh;
+    a.sf = (long)P.ny * P.nxh;
+    a.nx = P.nx;
+    a.ny = P.ny;
+    a.nz = P.nz;
+    a.dsym = h->dsym;
+    for (int i = 0; i < nb; i++) a.ops[i] = ops[b0 + i];
+    long total = (long)P.nxh * P.ny;
+    dim3 grid(nb, (unsigned)((total + P.wz - 1) / P.wz));
+    k_fft_z_conv<<<grid, kThreads, smem_yz(P.nz, P.wz), h->stream>>>(a);
+    HE4_LAUNCHED(h);
+  }
+  return HE4_OK;
+}
+
+int fft_z_only(Handle *h, double2 *buf, bool inverse) {
+  ZOp op{buf, buf, nullptr, 1.0, -1, inverse ? 2 : 1};
+  return fft_z_conv(h, 1, &op);
+}
+
+int fft_x_only(Handle *h, const double *rin, double2 *cout, const double2 *cin, double *rout, bool inverse) {
+  const FftPlan &P = h->fft;
+  XArgs a{};
+  a.ax = P.ax;
+  a.nxh = P.nxh;
+  a.P = P.px;
+  a.nrow = (long)P.ny * P.nz;
+  a.scale = 1.0;
+  a.rin[0] = rin;
+  a.cout[0] = cout;
+  a.cin[0] = cin;
+  a.rout[0] = rout;
+  dim3 grid((unsigned)((a.nrow + 2 * P.px - 1) / (2 * P.px)), 1);
+  if (inverse)
+    k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+  else
+    k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+}  // namespace he4

@@ -1,0 +1,395 @@
+// field.cu -- the mean-field evaluation: potenimp, poten (with term_alfa)
+// and forceimp (potenimp.f90:1-73, poten.f90:5-129, term_alfa.f90:5-117,
+// derden.f90:5-31, denpart/ironing potenimp.f90:294-371).
+//
+// Spectra: spec[0] holds the x/y-transformed density (fden before its z
+// transform) for the whole evaluation; forceimp reuses it, since for the
+// periodic stencils (icon=8) FFT(d_i rho) = i D_i(k) FFT(rho) exactly, D_i
+// being the symbol of the npd-point first-derivative stencil.
+#include "common.cuh"
+#include "stencil.cuh"
+
+namespace he4 {
+
+static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz}; }
+
+// ---------------------------------------------------------------------------
+// impurity density (denpart, potenimp.f90:294-338)
+// ---------------------------------------------------------------------------
+struct DepArgs {
+  int nx, ny, nz, npar;
+  double xmin, ymin, zmin, hx, hy, hz;
+};
+
+// NGP cell index as the reference computes it: int(1.5 + (r - r0)/h), 1-based
+__device__ __forceinline__ bool ngp_cell(const DepArgs &a, double rx, double ry, double rz, size_t *cell) {
+  const double fx = 1.5 + (rx - a.xmin) / a.hx;
+  const double fy = 1.5 + (ry - a.ymin) / a.hy;
+  const double fz = 1.5 + (rz - a.zmin) / a.hz;
+  if (!(fx > -1e9 && fx < 1e9 && fy > -1e9 && fy < 1e9 && fz > -1e9 && fz < 1e9)) return false;
+  const int ix = (int)fx, iy = (int)fy, iz = (int)fz;  // truncation toward zero
+  if (iz >= 1 && iz <= a.nz && iy >= 1 && iy <= a.ny && ix >= 1 && ix <= a.nx) {
+    *cell = ((size_t)(iz - 1) * a.ny + (iy - 1)) * a.nx + (ix - 1);
+    return true;
+  }
+  return false;
+}
+
+__global__ void k_deposit(const double *__restrict__ rimp, unsigned int *counts, DepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.npar) return;
+  size_t cell;
+  if (ngp_cell(a, rimp[p], rimp[a.npar + p], rimp[2 * a.npar + p], &cell)) atomicAdd(counts + cell, 1u);
+}
+
+// denx = count / N_par / hxyz (potenimp.f90:322)
+__global__ void k_denx(const unsigned int *__restrict__ counts, double *denx, size_t n, double npar, double hxyz) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) denx[t] = (double)counts[t] / npar / hxyz;
+}
+
+// ironing (ironing.f90:19-28): interior points get 1/12 * (6 neighbours) +
+// 1/2 * centre, boundary points are copied.  Optionally writes sqrt.
+__global__ void k_iron(const double *__restrict__ src, double *dst, double *sqrt_out, Geo g) {
+  HE4_IJK(g);
+  double v;
+  if (i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1) {
+    const size_t sy = g.nx, sz = (size_t)g.nx * g.ny;
+    const double s6 = ((((src[t - 1] + src[t + 1]) + src[t - sy]) + src[t + sy]) + src[t - sz]) + src[t + sz];
+    v = (1.0 / 12.0) * s6 + 0.5 * src[t];
+  } else {
+    v = src[t];
+  }
+  dst[t] = v;
+  if (sqrt_out) sqrt_out[t] = sqrt(v);
+}
+
+__global__ void k_sqrt(const double *__restrict__ src, double *dst, size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = sqrt(src[t]);
+}
+
+// out = scale * (d2x f + d2y f + d2z f)
+__global__ void k_lap_r(const double *__restrict__ f, double *out, double scale, Stencil st, Geo g) {
+  HE4_IJK(g);
+  const double a = stencil_axis(f, st.w2[0], st.m, g, i, j, k, 0);
+  const double b = stencil_axis(f, st.w2[1], st.m, g, i, j, k, 1);
+  const double c = stencil_axis(f, st.w2[2], st.m, g, i, j, k, 2);
+  out[t] = scale * ((a + b) + c);
+}
+
+// derden (derden.f90:26-28)
+__global__ void k_grad(const double *__restrict__ f, double *dx, double *dy, double *dz, Stencil st, Geo g) {
+  HE4_IJK(g);
+  dx[t] = stencil_axis(f, st.w1[0], st.m, g, i, j, k, 0);
+  dy[t] = stencil_axis(f, st.w1[1], st.m, g, i, j, k, 1);
+  dz[t] = stencil_axis(f, st.w1[2], st.m, g, i, j, k, 2);
+}
+
+// ---------------------------------------------------------------------------
+// poten pointwise pieces
+// ---------------------------------------------------------------------------
+struct OtArgs {
+  double cp4, cpp4, den0s, h2o2m4, alphas, c_solid, beta, den_m;
+};
+
+// sto1 = den*dencg*(cp4+cpp4*dencg) (poten.f90:62-64)
+__global__ void k_corr_src(const double *__restrict__ den, const double *__restrict__ dencg, double *out, size_t n,
+                           OtArgs a) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = den[t] * dencg[t] * (a.cp4 + a.cpp4 * dencg[t]);
+}
+
+// penalty (poten.f90:80-81) and pot4 = delj4 + dencg^2 (a0 + a1 dencg) + sto1 (poten.f90:88-92)
+__global__ void k_pot4_base(const double *__restrict__ den, const double *__restrict__ dencg,
+                            const double *__restrict__ delj4, const double *__restrict__ corr, double *penalty,
+                            double *pot4, size_t n, OtArgs a) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double d = den[t];
+  const double th = tanh(a.beta * (d - a.den_m));
+  penalty[t] = a.c_solid * (1.0 + th + a.beta * d * (1.0 - th * th));
+  const double dc = dencg[t];
+  const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0;
+  pot4[t] = delj4[t] + dc * dc * (a0 + a1 * dc) + corr[t];
+}
+
+// falfs = 1 - denalf/den0s; g_i = falfs * d_i rho (term_alfa.f90:28-36)
+__global__ void k_alfa1(const double *__restrict__ denalf, const double *__restrict__ dx,
+                        const double *__restrict__ dy, const double *__restrict__ dz, double *falfs, double *g0,
+                        double *g1, double *g2, size_t n, OtArgs a) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double f = 1.0 - denalf[t] / a.den0s;
+  falfs[t] = f;
+  g0[t] = f * dx[t];
+  g1[t] = f * dy[t];
+  g2[t] = f * dz[t];
+}
+
+// s = sum_i d_i rho * int_i ; h_i = falfs * int_i (term_alfa.f90:65-69, 87-92)
+__global__ void k_alfa2(const double *__restrict__ dx, const double *__restrict__ dy, const double *__restrict__ dz,
+                        const double *__restrict__ ix, const double *__restrict__ iy, const double *__restrict__ iz,
+                        const double *__restrict__ falfs, double *s, double *h0, double *h1, double *h2, size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  s[t] = (dx[t] * ix[t]) + (dy[t] * iy[t]) + (dz[t] * iz[t]);
+  const double f = falfs[t];
+  h0[t] = f * ix[t];
+  h1[t] = f * iy[t];
+  h2[t] = f * iz[t];
+}
+
+// ualphas = (u1/den0s + sum_i d_i h_i) * h2o2m4 * alphas ; pot4 += ualphas
+// (term_alfa.f90:110-113, poten.f90:101-104)
+__global__ void k_alfa3(double *ualphas, const double *__restrict__ h0, const double *__restrict__ h1,
+                        const double *__restrict__ h2, double *pot4, Stencil st, Geo g, OtArgs a) {
+  HE4_IJK(g);
+  const double d0 = stencil_axis(h0, st.w1[0], st.m, g, i, j, k, 0);
+  const double d1 = stencil_axis(h1, st.w1[1], st.m, g, i, j, k, 1);
+  const double d2 = stencil_axis(h2, st.w1[2], st.m, g, i, j, k, 2);
+  const double u = ualphas[t] / a.den0s;
+  const double ua = (u + d0 + d1 + d2) * a.h2o2m4 * a.alphas;
+  ualphas[t] = ua;
+  pot4[t] = pot4[t] + ua;
+}
+
+// pot4 = pot4 + uimp + penalty (poten.f90:122-124)
+__global__ void k_pot4_final(double *pot4, const double *__restrict__ uimp, const double *__restrict__ penalty,
+                             size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) pot4[t] = pot4[t] + uimp[t] + penalty[t];
+}
+
+// ---------------------------------------------------------------------------
+// forceimp pieces
+// ---------------------------------------------------------------------------
+// f_i = (f_i + (1/denx)(d_i psix * hpsix - psix * d_i hpsix)) / m_X where
+// denx > 0 (potenimp.f90:52-69)
+__global__ void k_force_q(double *fx, double *fy, double *fz, const double *__restrict__ psix,
+                          const double *__restrict__ hpsix, const double *__restrict__ denx, double minv_unused,
+                          double mass, Stencil st, Geo g) {
+  HE4_IJK(g);
+  const double dn = denx[t];
+  const double inv = (dn > 0.0) ? 1.0 / dn : 0.0;
+  const double ps = psix[t], hp = hpsix[t];
+  double *F[3] = {fx, fy, fz};
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++) {
+    const double dps = stencil_axis(psix, st.w1[ax], st.m, g, i, j, k, ax);
+    const double dhp = stencil_axis(hpsix, st.w1[ax], st.m, g, i, j, k, ax);
+    F[ax][t] = (F[ax][t] + inv * (dps * hp - ps * dhp)) / mass;
+  }
+}
+
+struct GatherArgs {
+  int nx, ny, nz, npar;
+  double x0, y0, z0, hx, hy, hz;
+};
+
+// trilinear blend of the 8 cell corners (blend_103, potenimp.f90:278-286)
+__device__ __forceinline__ double blend103(double r, double s, double t, double x000, double x001, double x010,
+                                           double x011, double x100, double x101, double x110, double x111) {
+  return 1.0 * (+x000) + r * (-x000 + x100) + s * (-x000 + x010) + t * (-x000 + x001) +
+         r * s * (+x000 - x100 - x010 + x110) + r * t * (+x000 - x100 - x001 + x101) +
+         s * t * (+x000 - x010 - x001 + x011) + r * s * t * (-x000 + x100 + x010 + x001 - x011 - x101 - x110 + x111);
+}
+
+// interpola3 (potenimp.f90:91-114): one thread per (particle, component)
+__global__ void k_gather(const double *__restrict__ rimp, const double *__restrict__ fx,
+                         const double *__restrict__ fy, const double *__restrict__ fz, double *aimp, GatherArgs a) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3 * a.npar) return;
+  const int c = gid / a.npar, p = gid - c * a.npar;
+  const double ax = (rimp[p] - a.x0) / a.hx + 1;
+  const double ay = (rimp[a.npar + p] - a.y0) / a.hy + 1;
+  const double az = (rimp[2 * a.npar + p] - a.z0) / a.hz + 1;
+  const bool ok = ax > -1e9 && ax < 1e9 && ay > -1e9 && ay < 1e9 && az > -1e9 && az < 1e9;
+  const int ix = ok ? (int)ax : 0, iy = ok ? (int)ay : 0, iz = ok ? (int)az : 0;
+  if (!ok || ix >= a.nx || iy >= a.ny || iz >= a.nz || ix <= 0 || iy <= 0 || iz <= 0) {
+    aimp[gid] = 0.0;
+    return;
+  }
+  const double r = ax - ix, s = ay - iy, tt = az - iz;
+  const double *f = (c == 0) ? fx : (c == 1) ? fy : fz;
+  auto G = [&](int ii, int jj, int kk) { return f[((size_t)(kk - 1) * a.ny + (jj - 1)) * a.nx + (ii - 1)]; };
+  aimp[gid] = blend103(r, s, tt, G(ix, iy, iz), G(ix, iy, iz + 1), G(ix, iy + 1, iz), G(ix, iy + 1, iz + 1),
+                       G(ix + 1, iy, iz), G(ix + 1, iy, iz + 1), G(ix + 1, iy + 1, iz),
+                       G(ix + 1, iy + 1, iz + 1));
+}
+
+// ---------------------------------------------------------------------------
+// orchestration
+// ---------------------------------------------------------------------------
+static OtArgs ot_args(const Handle *h) {
+  OtArgs a;
+  a.cp4 = h->p.cp4;
+  a.cpp4 = h->p.cpp4;
+  a.den0s = h->p.den0s;
+  a.h2o2m4 = h->p.h2o2m4;
+  a.alphas = h->p.alphas;
+  a.c_solid = h->p.c_solid;
+  a.beta = h->p.beta_solid;
+  a.den_m = h->p.den_m;
+  return a;
+}
+
+static inline unsigned nblk(size_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+int field_potenimp(Handle *h) {
+  const Geo g = geo(h);
+  const size_t N = h->N;
+  DepArgs d;
+  d.nx = h->nx;
+  d.ny = h->ny;
+  d.nz = h->nz;
+  d.npar = h->npar;
+  d.xmin = -h->p.xmax;
+  d.ymin = -h->p.ymax;
+  d.zmin = -h->p.zmax;
+  d.hx = h->hx;
+  d.hy = h->hy;
+  d.hz = h->hz;
+  HE4_CUDA_TRY(cudaMemsetAsync(h->counts, 0, sizeof(unsigned int) * N, h->stream));
+  k_deposit<<<nblk(h->npar), 256, 0, h->stream>>>(h->rimp, h->counts, d);
+  HE4_LAUNCHED(h);
+  const double hxyz = h->hx * h->hy * h->hz;
+  k_denx<<<nblk(N), 256, 0, h->stream>>>(h->counts, h->denx, N, (double)h->npar, hxyz);
+  HE4_LAUNCHED(h);
+  if (h->p.ironx <= 0) {
+    k_sqrt<<<nblk(N), 256, 0, h->stream>>>(h->denx, h->psix, N);
+    HE4_LAUNCHED(h);
+  } else {
+    for (int it = 0; it < h->p.ironx; it++) {
+      // ping-pong through rtmp[0]; the last pass lands in denx and writes psix
+      double *src = (it % 2 == 0) ? h->denx : h->rtmp[0];
+      double *dst = (it % 2 == 0) ? h->rtmp[0] : h->denx;
+      const bool last = (it == h->p.ironx - 1);
+      k_iron<<<grid3(g), block3(), 0, h->stream>>>(src, dst, last ? h->psix : nullptr, g);
+      HE4_LAUNCHED(h);
+      if (last && dst != h->denx) {
+        HE4_CUDA_TRY(cudaMemcpyAsync(h->denx, dst, sizeof(double) * N, cudaMemcpyDeviceToDevice, h->stream));
+      }
+    }
+  }
+  k_lap_r<<<grid3(g), block3(), 0, h->stream>>>(h->psix, h->hpsix, -h->h2o2mx, h->st, g);
+  HE4_LAUNCHED(h);
+  // uimp = IFFT(FFT(denx) * Vq) * renor (potenimp.f90:17-19)
+  const double *in[1] = {h->denx};
+  double2 *sp[1] = {h->spec[1]};
+  HE4_TRY(fft_r2c(h, 1, in, sp));
+  ZOp op{h->spec[1], h->spec[1], h->vq, h->renor, -1};
+  HE4_TRY(fft_z_conv(h, 1, &op));
+  double *out[1] = {h->uimp};
+  HE4_TRY(fft_c2r(h, 1, sp, out));
+  return HE4_OK;
+}
+
+int field_poten(Handle *h) {
+  const Geo g = geo(h);
+  const size_t N = h->N;
+  const OtArgs ot = ot_args(h);
+  const bool otc = (h->p.core4 == HE4_CORE_OTC);
+  // fden: x/y transform of den kept in spec[0] (poten.f90:27)
+  {
+    const double *in[1] = {h->den};
+    double2 *sp[1] = {h->spec[0]};
+    HE4_TRY(fft_r2c(h, 1, in, sp));
+  }
+  // dencg, delj4, (denalf): poten.f90:34-38, 46-50, 95-99
+  {
+    ZOp ops[3] = {{h->spec[0], h->spec[1], h->wcgk, h->renor, -1},
+                  {h->spec[0], h->spec[2], h->fvlj4, h->renor, -1},
+                  {h->spec[0], h->spec[3], h->kalfs, h->renor, -1}};
+    const int nop = otc ? 3 : 2;
+    HE4_TRY(fft_z_conv(h, nop, ops));
+    double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
+    double *out[3] = {h->dencg, h->delj4, h->denalf};
+    HE4_TRY(fft_c2r(h, nop, sp, out));
+  }
+  // derden
+  k_grad<<<grid3(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+  HE4_LAUNCHED(h);
+  // correlation convolution (poten.f90:62-74)
+  k_corr_src<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->rtmp[0], N, ot);
+  HE4_LAUNCHED(h);
+  {
+    const double *in[1] = {h->rtmp[0]};
+    double2 *sp[1] = {h->spec[1]};
+    HE4_TRY(fft_r2c(h, 1, in, sp));
+    ZOp op{h->spec[1], h->spec[1], h->wcgk, h->renor, -1};
+    HE4_TRY(fft_z_conv(h, 1, &op));
+    double *out[1] = {h->corr};
+    HE4_TRY(fft_c2r(h, 1, sp, out));
+  }
+  k_pot4_base<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->delj4, h->corr, h->penalty, h->pot4, N, ot);
+  HE4_LAUNCHED(h);
+  // term_alfa (term_alfa.f90:28-113), called for core4='OTC' only
+  // (poten.f90:94-105).
+  if (otc) {
+    k_alfa1<<<nblk(N), 256, 0, h->stream>>>(h->denalf, h->dxden, h->dyden, h->dzden, h->falfs, h->rtmp[0],
+                                           h->rtmp[1], h->rtmp[2], N, ot);
+    HE4_LAUNCHED(h);
+    {
+      const double *in[3] = {h->rtmp[0], h->rtmp[1], h->rtmp[2]};
+      double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
+      HE4_TRY(fft_r2c(h, 3, in, sp));
+      ZOp ops[3] = {{h->spec[1], h->spec[1], h->kalfs, h->renor, -1},
+                    {h->spec[2], h->spec[2], h->kalfs, h->renor, -1},
+                    {h->spec[3], h->spec[3], h->kalfs, h->renor, -1}};
+      HE4_TRY(fft_z_conv(h, 3, ops));
+      double *out[3] = {h->intx, h->inty, h->intz};
+      HE4_TRY(fft_c2r(h, 3, sp, out));
+    }
+    k_alfa2<<<nblk(N), 256, 0, h->stream>>>(h->dxden, h->dyden, h->dzden, h->intx, h->inty, h->intz, h->falfs,
+                                           h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], N);
+    HE4_LAUNCHED(h);
+    {
+      const double *in[1] = {h->rtmp[0]};
+      double2 *sp[1] = {h->spec[1]};
+      HE4_TRY(fft_r2c(h, 1, in, sp));
+      ZOp op{h->spec[1], h->spec[1], h->kalfs, h->renor, -1};
+      HE4_TRY(fft_z_conv(h, 1, &op));
+      double *out[1] = {h->ualphas};
+      HE4_TRY(fft_c2r(h, 1, sp, out));
+    }
+    k_alfa3<<<grid3(g), block3(), 0, h->stream>>>(h->ualphas, h->rtmp[1], h->rtmp[2], h->rtmp[3], h->pot4, h->st,
+                                                  g, ot);
+    HE4_LAUNCHED(h);
+  }
+  k_pot4_final<<<nblk(N), 256, 0, h->stream>>>(h->pot4, h->uimp, h->penalty, N);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+int field_forceimp(Handle *h) {
+  const Geo g = geo(h);
+  // f_i = -IFFT(FFT(d_i rho) Vq) * renor = IFFT(-renor Vq i D_i fden)
+  // (potenimp.f90:42-50)
+  ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, -h->renor, 0},
+                {h->spec[0], h->spec[2], h->vq, -h->renor, 1},
+                {h->spec[0], h->spec[3], h->vq, -h->renor, 2}};
+  HE4_TRY(fft_z_conv(h, 3, ops));
+  double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
+  double *out[3] = {h->fx, h->fy, h->fz};
+  HE4_TRY(fft_c2r(h, 3, sp, out));
+  k_force_q<<<grid3(g), block3(), 0, h->stream>>>(h->fx, h->fy, h->fz, h->psix, h->hpsix, h->denx, 0.0, h->mAg_u,
+                                                  h->st, g);
+  HE4_LAUNCHED(h);
+  GatherArgs a;
+  a.nx = h->nx;
+  a.ny = h->ny;
+  a.nz = h->nz;
+  a.npar = h->npar;
+  a.x0 = -h->p.xmax;
+  a.y0 = -h->p.ymax;
+  a.z0 = -h->p.zmax;
+  a.hx = h->hx;
+  a.hy = h->hy;
+  a.hz = h->hz;
+  k_gather<<<nblk(3 * (size_t)h->npar), 256, 0, h->stream>>>(h->rimp, h->fx, h->fy, h->fz, h->aimp, a);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+}  // namespace he4

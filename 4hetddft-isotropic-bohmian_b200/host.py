@@ -1,0 +1,178 @@
+"""Python host mirror of the C ABI (include/he4_tddft.h).
+
+The reference drives its time step through argument-less Fortran subroutines
+operating on module arrays (DFT4He3d.f90:630-634, 848-878): potenimp, poten,
+forceimp, steprk(deltat), steppc(deltat, errHe, errimp, errvimp), energy.
+`He4Step` exposes the same operations, with the same names and argument
+meaning, on a handle that owns the device state.  Errors raise `He4Error`
+carrying the library's code and message; nothing falls back to the CPU.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhe4b200.so")
+
+_lib = None
+
+
+class He4Error(RuntimeError):
+    def __init__(self, code, what, detail):
+        super().__init__(f"{what}: {detail} (code {code})")
+        self.code = code
+
+
+def load_library():
+    """Load libhe4b200.so; raises if the CUDA library has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `python {os.path.join(HERE, 'build.py')}`")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, i32 = C.c_void_p, C.POINTER(C.c_double), C.c_int32
+    L.he4_params_default.argtypes = [vp]
+    L.he4_params_default.restype = None
+    L.he4_create.argtypes = [vp, C.POINTER(vp)]
+    L.he4_destroy.argtypes = [vp]
+    L.he4_destroy.restype = None
+    L.he4_set_state.argtypes = [vp, dp, dp, dp]
+    L.he4_get_state.argtypes = [vp, dp, dp, dp, dp]
+    for n in ("he4_potenimp", "he4_poten", "he4_forceimp", "he4_field"):
+        getattr(L, n).argtypes = [vp]
+    L.he4_step_rk.argtypes = [vp, C.c_double, dp]
+    L.he4_step_pc.argtypes = [vp, C.c_double, dp, dp]
+    L.he4_run.argtypes = [vp, i32, C.c_double, dp, dp]
+    L.he4_energy.argtypes = [vp, vp]
+    L.he4_get_field.argtypes = [vp, i32, dp]
+    L.he4_get_kernel.argtypes = [vp, i32, dp]
+    L.he4_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.he4_launch_count.argtypes = [vp]
+    L.he4_launch_count.restype = C.c_int64
+    L.he4_strerror.argtypes = [C.c_int]
+    L.he4_strerror.restype = C.c_char_p
+    L.he4_last_error.argtypes = []
+    L.he4_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(code, what):
+    if code != 0:
+        L = load_library()
+        raise He4Error(code, what, (L.he4_last_error() or b"").decode() or L.he4_strerror(code).decode())
+
+
+def params_default():
+    """he4_params_default() from the library."""
+    p = abi.He4Params()
+    load_library().he4_params_default(C.byref(p))
+    return p
+
+
+class He4Step:
+    """Device-resident time step of one droplet + impurity system."""
+
+    def __init__(self, params):
+        L = load_library()
+        self.p = params
+        self._h = C.c_void_p()
+        _check(L.he4_create(C.byref(params), C.byref(self._h)), "he4_create")
+        self.shape = (params.nz, params.ny, params.nx)
+        self.hshape = (params.nz, params.ny, params.nx // 2 + 1)
+        self.npar = params.n_par
+
+    def close(self):
+        if self._h:
+            load_library().he4_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # readenc mode 2 / printoutc
+    def set_state(self, psi, rimp, vimp):
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        rimp = np.ascontiguousarray(rimp, dtype=np.float64)
+        vimp = np.ascontiguousarray(vimp, dtype=np.float64)
+        if psi.shape != self.shape or rimp.shape != (3, self.npar) or vimp.shape != (3, self.npar):
+            raise ValueError("state arrays do not match the grid / n_par")
+        _check(load_library().he4_set_state(self._h, _dp(psi.view(np.float64)), _dp(rimp), _dp(vimp)),
+               "he4_set_state")
+
+    def get_state(self):
+        psi = np.zeros(self.shape, dtype=np.complex128)
+        r, v, a = (np.zeros((3, self.npar)) for _ in range(3))
+        _check(load_library().he4_get_state(self._h, _dp(psi.view(np.float64)), _dp(r), _dp(v), _dp(a)),
+               "he4_get_state")
+        return psi, r, v, a
+
+    # field evaluation
+    def potenimp(self):
+        _check(load_library().he4_potenimp(self._h), "he4_potenimp")
+
+    def poten(self):
+        _check(load_library().he4_poten(self._h), "he4_poten")
+
+    def forceimp(self):
+        _check(load_library().he4_forceimp(self._h), "he4_forceimp")
+
+    def field(self):
+        _check(load_library().he4_field(self._h), "he4_field")
+
+    # time steps
+    def steprk(self, deltat):
+        m = np.zeros(9)
+        _check(load_library().he4_step_rk(self._h, deltat, _dp(m)), "he4_step_rk")
+        return m
+
+    def steppc(self, deltat):
+        e, m = np.zeros(3), np.zeros(9)
+        _check(load_library().he4_step_pc(self._h, deltat, _dp(e), _dp(m)), "he4_step_pc")
+        return e, m
+
+    def run(self, nsteps, deltat):
+        e, m = np.zeros((nsteps, 3)), np.zeros((nsteps, 9))
+        _check(load_library().he4_run(self._h, nsteps, deltat, _dp(e), _dp(m)), "he4_run")
+        return e, m
+
+    def energy(self):
+        E = abi.He4Energies()
+        _check(load_library().he4_energy(self._h, C.byref(E)), "he4_energy")
+        return E.as_dict()
+
+    def get_field(self, name):
+        out = np.zeros(self.shape)
+        _check(load_library().he4_get_field(self._h, abi.FIELD_ID[name], _dp(out)), "he4_get_field")
+        return out
+
+    def get_kernel(self, name):
+        out = np.zeros(self.hshape)
+        _check(load_library().he4_get_kernel(self._h, abi.KERNEL_ID[name], _dp(out)), "he4_get_kernel")
+        return out
+
+    def stream(self):
+        s = C.c_void_p()
+        _check(load_library().he4_get_stream(self._h, C.byref(s)), "he4_get_stream")
+        return s.value
+
+    def launch_count(self):
+        return int(load_library().he4_launch_count(self._h))

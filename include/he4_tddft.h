@@ -1,0 +1,179 @@
+/*
+ * he4_tddft.h -- C ABI of the B200 time-step library for the Orsay-Trento
+ * time-dependent 4He density functional with a Bohmian test-particle impurity.
+ *
+ * The reference program (Fortran 90, DFT4He3d.f90) keeps all state in module
+ * variables and calls argument-less subroutines.  This header replaces the
+ * per-time-step calls of its main loop with explicit entry points on a handle
+ * that owns every device array.  The Fortran host keeps the namelist parsing
+ * (DFT4He3d.f90:147-187), readenc/printoutc file I/O and diagnostics and binds
+ * these functions through ISO_C_BINDING (see INTEGRATION.md for the interface
+ * block).
+ *
+ * Conventions
+ *  - Grid arrays are x-fastest: C [nz][ny][nx] == Fortran a(nx,ny,nz).
+ *  - Complex arrays are interleaved (re,im) doubles == Fortran complex(8).
+ *  - Particle arrays are [3][n_par] == Fortran rimp(N_par,3).
+ *  - Every function returns HE4_OK (0) or a negative HE4_E_* code; nothing
+ *    aborts the host process.  he4_strerror() turns a code into text, and
+ *    he4_last_error() returns the detail message of the last failing call on
+ *    this thread.
+ *  - One host thread per handle; handles are independent.
+ */
+#ifndef HE4_TDDFT_H
+#define HE4_TDDFT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HE4_OK 0
+#define HE4_E_ARG (-1)         /* invalid argument or parameter            */
+#define HE4_E_UNSUPPORTED (-2) /* valid in the reference, not implemented   */
+#define HE4_E_NOMEM (-3)       /* device or host allocation failed          */
+#define HE4_E_CUDA (-4)        /* a CUDA runtime call failed                */
+#define HE4_E_STATE (-5)       /* call order violated (e.g. no state set)   */
+#define HE4_E_NONFINITE (-6)   /* a returned scalar is NaN or inf           */
+#define HE4_E_NODEVICE (-7)    /* no usable sm_100 device                   */
+
+/* core4 of the namelist (modules.f90:210): 'OT ' or 'OTC'. */
+enum { HE4_CORE_OT = 0, HE4_CORE_OTC = 1 };
+
+/* Source of the impurity pair-potential kernel Vq (DFT4He3d.f90:527-536). */
+enum {
+  HE4_POT_TABLE = 0, /* caller supplies Vq on the half-spectrum grid        */
+  HE4_POT_MORSE = 1, /* V(r)=D[(1-exp(-a(r-re)))^2-1], r<r_cutoff -> umax,  */
+                     /* transformed by the FT_V_spline procedure           */
+  HE4_POT_NULL = 2   /* V = 0 ('null' entry of Select_Pot)                  */
+};
+
+/* Arithmetic of the convolution FFTs and the pointwise potential assembly. */
+enum { HE4_PREC_FP64 = 0 };
+
+typedef struct he4_params {
+  /* grid (namelist nx,ny,nz,xmax,ymax,zmax; DFT4He3d.f90:271-354) */
+  int32_t nx, ny, nz;
+  double xmax, ymax, zmax;
+  /* derivatives (module deriva): npd odd in [3,25]; icon 8 = periodic */
+  int32_t npd, icon;
+  /* functional */
+  int32_t core4;
+  double cp4, cpp4, den4c, alphas, l_alfs, den0s, h2o2m4;
+  double c_solid, beta_solid, den_m; /* penalty C, beta, den_m (he4 module) */
+  double eps4, sigma4, b4, h4;       /* screened LJ (lenard4), h4 = core   */
+  /* impurity */
+  int32_t n_par;  /* number of Bohmian test particles                     */
+  int32_t ironx;  /* number of 7-point smoothings of denx (field module)  */
+  double mimpur;  /* impurity mass in amu                                  */
+  int32_t pot_kind;
+  double morse_d, morse_alpha, morse_re, r_cutoff, umax;
+  int32_t nq;              /* q-points of the FT_V_spline table            */
+  const double *vq_table;  /* HE4_POT_TABLE: [nz][ny][nx/2+1] real values  */
+  /* absorbing layer timec = (Lambdah(1+tanh((z-tzmean)/tzsurf)), 1) */
+  double lambdah, tzmean, tzsurf;
+  int32_t precision;
+  int32_t device; /* CUDA device ordinal                                   */
+} he4_params;
+
+/* Energies of energy.f90:51-124, same names as module energies. */
+typedef struct he4_energies {
+  double etot, etot4, ekin4, elj4, ecor4, ealphas, esolid;
+  double ekinx, ekinqx, eHeX, eimpu;
+} he4_energies;
+
+/* Real grid fields readable with he4_get_field (module arrays). */
+enum {
+  HE4_F_DEN = 0, HE4_F_POT4, HE4_F_DENX, HE4_F_PSIX, HE4_F_HPSIX, HE4_F_UIMP,
+  HE4_F_DENCG, HE4_F_DELJ4, HE4_F_DENALF, HE4_F_UALPHAS, HE4_F_FALFS,
+  HE4_F_INTXALF, HE4_F_INTYALF, HE4_F_INTZALF, HE4_F_DXDEN, HE4_F_DYDEN,
+  HE4_F_DZDEN, HE4_F_FX, HE4_F_FY, HE4_F_FZ, HE4_F_PENALTY, HE4_F_CORR,
+  HE4_F_COUNT
+};
+
+/* Half-spectrum kernels [nz][ny][nx/2+1] readable with he4_get_kernel. */
+enum { HE4_K_WCGK = 0, HE4_K_FVLJ4, HE4_K_KALFS, HE4_K_VQ, HE4_K_PMOD,
+       HE4_K_COUNT };
+
+typedef struct he4_handle he4_handle;
+
+/* Fill p with the reference defaults (modules.f90:15-19,81-90,124-139,
+ * 144,205-210; DFT4He3d.f90:184-186). */
+void he4_params_default(he4_params *p);
+
+/* Replaces dimen (dimen.f90:29-143), fftini (fft.f90:5-76), Init_deriv_p
+ * (init_deriv_parallel.f90:51-85) and the kernel construction of
+ * DFT4He3d.f90:509-570 (fforma, FT_V_spline, initcg, kalfs). */
+int he4_create(const he4_params *p, he4_handle **out);
+void he4_destroy(he4_handle *h);
+
+/* readenc mode 2 (readenc.f90:96-114): psi [nz][ny][nx] complex, rimp and
+ * vimp [3][n_par].  Also sets den=|psi|^2 (readenc.f90:102), zeroes the
+ * RK/PC histories (dimen.f90:75-79,133-134; DFT4He3d.f90:841-845) and makes
+ * the next he4_run/he4_step call start with the RK-Gill starter. */
+int he4_set_state(he4_handle *h, const double *psi, const double *rimp,
+                  const double *vimp);
+/* printoutc inputs (printoutc.f90:139-142) plus aimp. Any pointer may be NULL. */
+int he4_get_state(he4_handle *h, double *psi, double *rimp, double *vimp,
+                  double *aimp);
+
+/* Field evaluation pieces: potenimp (potenimp.f90:1-20), poten
+ * (poten.f90:5-129), forceimp (potenimp.f90:24-73), and all three in that
+ * order (DFT4He3d.f90:630-634, 861-863). */
+int he4_potenimp(he4_handle *h);
+int he4_poten(he4_handle *h);
+int he4_forceimp(he4_handle *h);
+int he4_field(he4_handle *h);
+
+/* One time step followed by the field evaluation of DFT4He3d.f90:861-863.
+ * he4_step_rk = steprk (steprk.f90:1-128); he4_step_pc = steppc
+ * (steppc.f90:1-155) and returns errHe, errimp, errvimp in err[3].
+ * means[9] (nullable) = <rimp>,<vimp>,<aimp> per axis after the field
+ * evaluation, internal units (DFT4He3d.f90:864-878). */
+int he4_step_rk(he4_handle *h, double deltat, double means[9]);
+int he4_step_pc(he4_handle *h, double deltat, double err[3], double means[9]);
+
+/* The iteration loop of DFT4He3d.f90:848-863 for nsteps steps: the first
+ * three steps after he4_set_state use steprk, the rest steppc (lrk=false).
+ * err [nsteps][3] (zeros for RK steps) and means [nsteps][9] are nullable.
+ * Runs from a captured CUDA graph after the first PC step. */
+int he4_run(he4_handle *h, int32_t nsteps, double deltat, double *err,
+            double *means);
+
+/* energy() (energy.f90:12-129) evaluated on the current fields. */
+int he4_energy(he4_handle *h, he4_energies *e);
+
+/* Copy-out of a real grid field ([nz][ny][nx]) or a half-spectrum kernel. */
+int he4_get_field(he4_handle *h, int32_t which, double *out);
+int he4_get_kernel(he4_handle *h, int32_t which, double *out);
+
+/* The handle's 3D real FFT on host buffers (same transform as the
+ * convolutions use; FFTW r2c/c2r conventions of fft.f90:43-65):
+ * in [nz][ny][nx] real -> out [nz][ny][nx/2+1] complex, unnormalised, and
+ * back (unnormalised: c2r(r2c(f)) = N f). */
+int he4_fft_r2c(he4_handle *h, const double *in, double *out);
+int he4_fft_c2r(he4_handle *h, const double *in, double *out);
+
+/* Measurement hook: launches one kernel of the step `reps` times on the
+ * handle's current buffers between two CUDA events on the handle's stream.
+ * which: 0 z-pass convolution (FFT_z, kernel multiply, IFFT_z), 1 y pass,
+ * 2 x pass R2C, 3 x pass C2R.  They only touch FFT scratch buffers.  Returns
+ * the mean time per launch, the algorithmic bytes one launch moves (each
+ * input read once, each output written once) and the kernel's name. */
+int he4_bench_kernel(he4_handle *h, int32_t which, int32_t reps, double *ms_per_launch,
+                     double *bytes_per_launch, char *name, int32_t name_len);
+
+/* Stream the handle launches on (cudaStream_t), for event timing. */
+int he4_get_stream(he4_handle *h, void **stream);
+/* Number of kernels this handle has launched (graph launches count the
+ * kernels inside the graph). */
+int64_t he4_launch_count(he4_handle *h);
+
+const char *he4_strerror(int code);
+const char *he4_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HE4_TDDFT_H */

@@ -1,0 +1,115 @@
+"""Host-side tests of the C ABI library (no GPU needed): the library loads,
+exports every function declared in include/he4_tddft.h, its structs match
+the ctypes mirror, its defaults match the reference modules, and without a
+usable device every entry point returns an error code instead of aborting."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "he4_tddft.h")
+
+
+@pytest.fixture(scope="module")
+def lib(pkg):
+    path = pkg.host.LIB_PATH
+    if not os.path.exists(path):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("he4_build", os.path.join(os.path.dirname(path), "build.py"))
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        m.build()
+    return pkg.load_library()
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(he4_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_function(lib):
+    names = declared_functions()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", lib._name], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT\s+(he4_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+
+
+def test_struct_layout_matches_header(pkg):
+    code = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "he4_tddft.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(he4_params), sizeof(he4_energies),
+         offsetof(he4_params, vq_table), offsetof(he4_params, lambdah),
+         offsetof(he4_params, device), offsetof(he4_params, nq));
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(src, "w").write(code)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+        got = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
+    P, E = pkg.abi.He4Params, pkg.abi.He4Energies
+    want = [C.sizeof(P), C.sizeof(E), P.vq_table.offset, P.lambdah.offset, P.device.offset, P.nq.offset]
+    assert got == want
+
+
+def test_defaults_match_reference_modules(pkg, lib):
+    p = pkg.params_default()
+    q = pkg.abi.default_params()
+    for name, _ in pkg.abi.He4Params._fields_:
+        if name == "vq_table":
+            continue
+        assert getattr(p, name) == getattr(q, name), name
+    # modules.f90:15,19,88-90,130-139,144,205-210
+    assert (p.npd, p.icon, p.nx, p.n_par) == (7, 8, 64, 100000)
+    assert (p.cp4, p.cpp4, p.alphas, p.den0s, p.h2o2m4) == (-2.41186e4, 1.85850e6, 54.31, 0.04, 6.05969638298)
+    assert (p.h4, p.eps4, p.sigma4, p.b4) == (2.190323, 10.22, 2.556, -718.99)
+
+
+def test_errors_are_codes_not_aborts(pkg, lib):
+    abi = pkg.abi
+    h = C.c_void_p()
+    p = pkg.params_default()
+    # invalid grid size: rejected before any device call
+    p.nx = 7
+    rc = lib.he4_create(C.byref(p), C.byref(h))
+    assert rc == abi.HE4_E_ARG and not h.value
+    assert b"grid" in lib.he4_last_error()
+    # icon other than 8 is not implemented
+    p = pkg.params_default()
+    p.icon = 13
+    assert lib.he4_create(C.byref(p), C.byref(h)) == abi.HE4_E_UNSUPPORTED
+    # null handle everywhere
+    assert lib.he4_field(None) == abi.HE4_E_ARG
+    assert lib.he4_step_pc(None, 1e-4, None, None) == abi.HE4_E_ARG
+    assert lib.he4_create(None, C.byref(h)) == abi.HE4_E_ARG
+    assert lib.he4_strerror(abi.HE4_E_NODEVICE) == b"no sm_100 device"
+
+
+def test_create_without_device_fails_cleanly(pkg, lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = pkg.params_default()
+    h = C.c_void_p()
+    rc = lib.he4_create(C.byref(p), C.byref(h))
+    assert rc in (pkg.abi.HE4_E_NODEVICE, pkg.abi.HE4_E_CUDA)
+    assert not h.value
+
+
+def test_oracle_rejects_what_the_library_rejects(pkg, ora):
+    p = pkg.abi.default_params()
+    p.icon = 13
+    with pytest.raises(ora.OracleError):
+        ora.Oracle(p)

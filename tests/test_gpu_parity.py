@@ -1,0 +1,189 @@
+"""GPU parity tests: the CUDA library (through its C ABI) against the CPU
+oracle on the same seeded inputs.
+
+Tolerances (FP64 everywhere):
+  * k-space kernels: pmod bit-identical; wcgk, kalfs 1e-14 and fvlj4 1e-11
+    relative to the largest value (different sin/cos/exp implementations);
+    Vq (single-precision values) within one FP32 ulp.
+  * one field evaluation: every field within 1e-11 of its largest value.
+  * energies after a field evaluation: 1e-10 relative per component.
+  * 3 RK + 10 PC steps: energy components and the norm 1e-10 relative, psi
+    within 1e-10 of its largest value, trajectory means 1e-9 relative.
+Integer work (the NGP deposit counts) must match exactly.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    s = max(np.max(np.abs(b)), 1e-300)
+    return float(np.max(np.abs(a - b)) / s)
+
+
+@pytest.fixture(scope="module")
+def c1(pkg, ora):
+    """64^3 droplet + 256 particles (the small benchmark configuration)."""
+    p, psi, r, v, _ = pkg.workloads.workload("c1")
+    o = ora.Oracle(p)
+    vq = o.get_kernel("vq")
+    return p, psi, r, v, o, vq
+
+
+def gpu_with_table(pkg, p, vq):
+    import ctypes as C
+    q = pkg.abi.He4Params.from_buffer_copy(p)
+    q.pot_kind = pkg.abi.HE4_POT_TABLE
+    vq = np.ascontiguousarray(vq)
+    q.vq_table = vq.ctypes.data_as(C.POINTER(C.c_double))
+    g = pkg.He4Step(q)
+    return g
+
+
+def test_kspace_kernels(pkg, c1):
+    p, psi, r, v, o, vq = c1
+    with pkg.He4Step(p) as g:
+        assert np.array_equal(g.get_kernel("pmod"), o.get_kernel("pmod"))
+        assert rel(g.get_kernel("wcgk"), o.get_kernel("wcgk")) < 1e-14
+        assert rel(g.get_kernel("kalfs"), o.get_kernel("kalfs")) < 1e-14
+        assert rel(g.get_kernel("fvlj4"), o.get_kernel("fvlj4")) < 1e-11
+        gv = g.get_kernel("vq")
+        # both are single-precision numbers; at most one FP32 ulp apart
+        ulp = np.spacing(np.abs(vq).astype(np.float32)).astype(np.float64)
+        assert np.all(np.abs(gv - vq) <= ulp)
+        assert np.mean(gv == vq) > 0.99
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 80), (48, 40, 30)])
+def test_fft_against_numpy_and_cufft(pkg, shape):
+    import ctypes as C
+    import torch
+    nx, ny, nz = shape
+    p = pkg.workloads.make_params(nx, 0.5, 8, pot=pkg.abi.HE4_POT_NULL, ny=ny, nz=nz)
+    rng = np.random.default_rng(11)
+    a = rng.standard_normal((nz, ny, nx))
+    with pkg.He4Step(p) as g:
+        L = pkg.load_library()
+        out = np.zeros((nz, ny, nx // 2 + 1), dtype=np.complex128)
+        dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+        assert L.he4_fft_r2c(g._h, dp(a), dp(out.view(np.float64))) == 0
+        want = np.fft.rfftn(a)
+        assert rel(out, want) < 1e-14
+        cufft = torch.fft.rfftn(torch.from_numpy(a).cuda()).cpu().numpy()
+        assert rel(out, cufft) < 1e-14
+        back = np.zeros_like(a)
+        assert L.he4_fft_c2r(g._h, dp(want.view(np.float64)), dp(back)) == 0
+        assert rel(back / a.size, a) < 1e-14
+
+
+def test_field_parity(pkg, c1):
+    p, psi, r, v, o, vq = c1
+    o.set_state(psi, r, v)
+    o.field()
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        g.field()
+        # integer deposit: identical impurity density
+        assert np.array_equal(g.get_field("denx"), o.get_field("denx"))
+        for name in pkg.abi.FIELDS:
+            assert rel(g.get_field(name), o.get_field(name)) < 1e-11, name
+        _, _, _, ag = g.get_state()
+        _, _, _, ao = o.get_state()
+        assert rel(ag, ao) < 1e-11
+        eg, eo = g.energy(), o.energy()
+        for k in eo:
+            assert abs(eg[k] - eo[k]) <= 1e-10 * max(abs(eo[k]), 1e-30), (k, eg[k], eo[k])
+
+
+def test_steps_parity(pkg, c1):
+    p, psi, r, v, o, vq = c1
+    dt = pkg.workloads.deltat_fs(1.0)
+    o.set_state(psi, r, v)
+    eo, mo = o.run(13, dt)
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        eg, mg = g.run(13, dt)
+        assert np.all(eg[:3] == 0) and np.all(eo[:3] == 0)
+        assert np.allclose(eg[3:], eo[3:], rtol=1e-8, atol=0)
+        assert np.allclose(mg, mo, rtol=1e-9, atol=1e-9 * np.abs(mo).max())
+        psg, rg, vg, ag = g.get_state()
+        pso, ro, vo, ao = o.get_state()
+        assert rel(psg, pso) < 1e-10
+        assert rel(rg, ro) < 1e-12 and rel(vg, vo) < 1e-10
+        Eg, Eo = g.energy(), o.energy()
+        for k in Eo:
+            assert abs(Eg[k] - Eo[k]) <= 1e-10 * max(abs(Eo[k]), 1e-30), (k, Eg[k], Eo[k])
+        dxyz = (2 * p.xmax / p.nx) ** 3
+        ng = np.sum(g.get_field("den")) * dxyz
+        no = np.sum(o.get_field("den")) * dxyz
+        assert abs(ng - no) <= 1e-10 * no
+
+
+def test_run_equals_single_steps_and_is_deterministic(pkg, c1):
+    p, psi, r, v, o, vq = c1
+    dt = pkg.workloads.deltat_fs(1.0)
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        e1, m1 = g.run(6, dt)
+        s1 = g.get_state()[0]
+        g.set_state(psi, r, v)
+        ms = [g.steprk(dt) for _ in range(3)]
+        es = []
+        for _ in range(3):
+            e, m = g.steppc(dt)
+            es.append(e)
+            ms.append(m)
+        s2 = g.get_state()[0]
+        assert np.array_equal(s1, s2)
+        assert np.array_equal(np.array(ms), m1)
+        assert np.array_equal(np.array(es), e1[3:])
+
+
+@pytest.mark.parametrize("variant", ["npd13", "ot_core", "noncubic"])
+def test_field_parity_variants(pkg, ora, variant):
+    w = pkg.workloads
+    if variant == "npd13":
+        p = w.make_params(48, 0.6, 64, npd=13)
+    elif variant == "ot_core":
+        p = w.make_params(48, 0.6, 64, core4=pkg.abi.HE4_CORE_OT)
+    else:
+        p = w.make_params(40, 0.6, 64, ny=48, nz=60)
+    psi = w.droplet_psi(p, 150)
+    r, v = w.particles(p.n_par, 5, 100.0)
+    o = ora.Oracle(p)
+    vq = o.get_kernel("vq")
+    o.set_state(psi, r, v)
+    o.field()
+    dt = w.deltat_fs(1.0)
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        g.field()
+        names = ["pot4", "dencg", "delj4", "uimp", "fx", "fy", "fz", "hpsix"]
+        if variant != "ot_core":
+            names += ["ualphas", "intxalf"]
+        for name in names:
+            assert rel(g.get_field(name), o.get_field(name)) < 1e-11, name
+        eg, _ = g.run(5, dt)
+        eo, _ = o.run(5, dt)
+        assert np.allclose(eg, eo, rtol=1e-8, atol=0)
+        Eg, Eo = g.energy(), o.energy()
+        for k in Eo:
+            assert abs(Eg[k] - Eo[k]) <= 1e-10 * max(abs(Eo[k]), 1e-30), (k, Eg[k], Eo[k])
+    o.close()
+
+
+def test_launch_count_and_errors(pkg, c1):
+    p, psi, r, v, o, vq = c1
+    with pkg.He4Step(p) as g:
+        with pytest.raises(pkg.He4Error) as ei:
+            g.field()  # no state yet
+        assert ei.value.code == pkg.abi.HE4_E_STATE
+        g.set_state(psi, r, v)
+        n0 = g.launch_count()
+        g.field()
+        assert g.launch_count() > n0
+        with pytest.raises(pkg.He4Error):
+            g.steppc(float("nan"))

@@ -1,0 +1,201 @@
+"""Pinning tests of the CPU oracle (no GPU).
+
+The reference ships no tests or golden outputs, so the oracle is pinned
+piece by piece: the stencil weights against the reference's own Bickley table
+(golden fixture from mates.f), the FFT against numpy's pocketfft, the sine
+integral against scipy, the spline against its defining conditions, the
+k-space kernels against analytic values and numerical quadrature, and the
+stencils against their Fourier symbols.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.integrate
+import scipy.special
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def test_fd_weights_match_reference_table_bitwise(ora):
+    rows = json.load(open(os.path.join(HERE, "golden", "blkds_central.json")))["rows"]
+    assert len(rows) == 24
+    for key, hexes in rows.items():
+        npd, order = map(int, key.split("_"))
+        want = np.array([float.fromhex(h) for h in hexes])
+        got = ora.fd_weights(npd, order)
+        assert np.array_equal(got, want), (key, got - want)
+
+
+@pytest.mark.parametrize("shape", [(8, 6, 10), (12, 9, 16), (16, 16, 16), (5, 8, 15), (32, 24, 20)])
+def test_fft_r2c_c2r_against_numpy(ora, shape):
+    rng = np.random.default_rng(7)
+    a = rng.standard_normal(shape)
+    got = ora.fft3_r2c(a)
+    want = np.fft.rfftn(a)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+    back = ora.fft3_c2r(want, shape[2])
+    n = a.size
+    assert np.max(np.abs(back / n - a)) <= 1e-13 * np.max(np.abs(a))
+
+
+def test_fft_c2r_ignores_dc_and_nyquist_imaginary_parts(ora):
+    # FFTW's c2r treats the input as the half of a Hermitian array: on the DC
+    # and Nyquist planes along x, a component whose (y,z) inverse transform is
+    # imaginary carries no information and must not change the output.
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((6, 6, 8))
+    s = np.fft.rfftn(a)
+    s2 = s.copy()
+    s2[..., 0] += 1j * np.fft.fft2(rng.standard_normal(s.shape[:2]))
+    s2[..., -1] += 1j * np.fft.fft2(rng.standard_normal(s.shape[:2]))
+    b1 = ora.fft3_c2r(s, 8)
+    b2 = ora.fft3_c2r(s2, 8)
+    assert np.allclose(b1, b2, rtol=0, atol=1e-12)
+
+
+def test_sine_integral_against_scipy(ora):
+    xs = np.concatenate([np.linspace(-30, 30, 601), [1e-8, 3.999, 4.0, 4.001, 16.0, 100.0, 1e4]])
+    for x in xs:
+        want = scipy.special.sici(x)[0]
+        assert abs(ora.si(x) - want) <= 2e-15 * max(1.0, abs(want)), x
+
+
+def test_spline_interpolates_with_given_end_curvatures(ora):
+    x = np.linspace(0.3, 4.0, 40)
+    y = np.sin(x) * np.exp(-x / 3)
+    s1, sn = -0.7, 0.2
+    a, b, c, d = ora.spline(x, y, s1, sn)
+    poly = lambda k, t: a[k] + t * (b[k] + t * (c[k] + t * d[k]))
+    d1 = lambda k, t: b[k] + t * (2 * c[k] + t * 3 * d[k])
+    d2 = lambda k, t: 2 * c[k] + 6 * d[k] * t
+    for k in range(len(x) - 1):
+        assert poly(k, x[k]) == pytest.approx(y[k], abs=1e-11)
+        assert poly(k, x[k + 1]) == pytest.approx(y[k + 1], abs=1e-11)
+    for k in range(len(x) - 2):
+        assert d1(k, x[k + 1]) == pytest.approx(d1(k + 1, x[k + 1]), abs=1e-9)
+        assert d2(k, x[k + 1]) == pytest.approx(d2(k + 1, x[k + 1]), abs=1e-8)
+    assert d2(0, x[0]) == pytest.approx(s1, abs=1e-8)
+    assert d2(len(x) - 2, x[-1]) == pytest.approx(sn, abs=1e-8)
+
+
+@pytest.fixture(scope="module")
+def small(pkg, ora):
+    p = pkg.workloads.make_params(16, 0.6, 8, pot=pkg.abi.HE4_POT_MORSE, nq=200)
+    o = ora.Oracle(p)
+    yield p, o
+    o.close()
+
+
+def _pz(p):
+    return 1.0 / (p.nz * 2.0 * p.zmax / p.nz)
+
+
+def test_kernels_analytic(pkg, small):
+    p, o = small
+    pm = o.get_kernel("pmod")
+    w = o.get_kernel("wcgk")
+    ka = o.get_kernel("kalfs")
+    assert w[0, 0, 0] == 1.0 and ka[0, 0, 0] == 1.0
+    a = 2 * math.pi * pm[1:, 0, 0] * p.h4
+    assert np.allclose(w[1:, 0, 0], 3 * (np.sin(a) - a * np.cos(a)) / a ** 3, rtol=1e-14, atol=1e-16)
+    assert np.allclose(ka, np.exp(-(math.pi * p.l_alfs * pm) ** 2), rtol=1e-14, atol=0)
+    # p grid: hpz = 1/(nz hz); pz(nz/2+1) = +pmax (DFT4He3d.f90:336-342)
+    hpz = _pz(p)
+    assert pm[1, 0, 0] == pytest.approx(hpz, rel=1e-15)
+    assert pm[p.nz // 2, 0, 0] == pytest.approx(p.nz / 2 * hpz, rel=1e-15)
+    assert pm[p.nz - 1, 0, 0] == pytest.approx(hpz, rel=1e-12)
+
+
+def test_fvlj4_zero_is_bforce_and_matches_quadrature(pkg, small):
+    p, o = small
+    f = o.get_kernel("fvlj4")
+    pm = o.get_kernel("pmod")
+    eps, sig, hc = p.eps4, p.sigma4, p.h4
+    b0 = 4 * math.pi * 4 * eps * (sig ** 12 / (9 * hc ** 9) - sig ** 6 / (3 * hc ** 3))
+    assert f[0, 0, 0] == pytest.approx(b0, rel=1e-14)
+    assert b0 == pytest.approx(p.b4, rel=1e-3)  # the check bforce exists for (fforma.f90:250-255)
+
+    def ft(pv):  # (2/p) int_hc^inf r V(r) sin(2 pi p r) dr, OT core (V=0 inside hc)
+        q = 2 * math.pi * pv
+        g = lambda r: 4 * eps * ((sig / r) ** 12 - (sig / r) ** 6) * r
+        val, _ = scipy.integrate.quad(g, hc, np.inf, weight="sin", wvar=q, limlst=200)
+        return 2.0 / pv * val
+
+    for idx in [(1, 0, 0), (2, 3, 1), (5, 1, 4), (8, 8, 8)]:
+        pv = pm[idx]
+        assert f[idx] == pytest.approx(ft(pv), rel=1e-8, abs=1e-9 * abs(b0))
+
+
+def test_vq_matches_quadrature_of_capped_morse(pkg, small):
+    p, o = small
+    vq = o.get_kernel("vq")
+    pm = o.get_kernel("pmod")
+    D, al, re_, rc, um = p.morse_d, p.morse_alpha, p.morse_re, p.r_cutoff, p.umax
+
+    def V(r):
+        return um if r < rc else D * ((1 - math.exp(-al * (r - re_))) ** 2 - 1)
+
+    def ft(pv):
+        if pv == 0:
+            inner = um * rc ** 3 / 3
+            outer, _ = scipy.integrate.quad(lambda r: r * r * V(r), rc, 200, limit=400)
+            return 4 * math.pi * (inner + outer)
+        q = 2 * math.pi * pv
+        inner, _ = scipy.integrate.quad(lambda r: r * um, 0, rc, weight="sin", wvar=q)
+        outer, _ = scipy.integrate.quad(lambda r: r * V(r), rc, 200, weight="sin", wvar=q, limit=2000)
+        return 4 * math.pi / q * (inner + outer)
+
+    scale = abs(vq[0, 0, 0])
+    for idx in [(0, 0, 0), (1, 0, 0), (3, 2, 1), (6, 5, 4), (8, 8, 8)]:
+        want = ft(pm[idx])
+        # FP32 rounding of cmplx() plus the q-spline interpolation error
+        assert vq[idx] == pytest.approx(want, rel=2e-5, abs=2e-5 * scale), idx
+    # values are single-precision numbers (DFT4He3d.f90:533)
+    assert np.array_equal(vq, vq.astype(np.float32).astype(np.float64))
+
+
+def test_periodic_stencils_match_fourier_symbol(pkg, ora, small):
+    p, o = small
+    n = p.nx
+    h = 2 * p.xmax / n
+    x = -p.xmax + h * np.arange(n)
+    for k in (1, 3, 5):
+        th = 2 * math.pi * k / n
+        f = np.broadcast_to(np.cos(th * np.arange(n)), (p.nz, p.ny, n)).copy()
+        w1 = ora.fd_weights(p.npd, 1)
+        w2 = ora.fd_weights(p.npd, 2)
+        m = p.npd // 2
+        s1 = 2 * sum(w1[m + t] * math.sin(th * t) for t in range(1, m + 1)) / h
+        s2 = (w2[m] + 2 * sum(w2[m + t] * math.cos(th * t) for t in range(1, m + 1))) / (h * h)
+        d1 = o.deriv(f, 1, 0)
+        d2 = o.deriv(f, 2, 0)
+        base = np.arange(n)
+        assert np.allclose(d1[0, 0], -s1 * np.sin(th * base), atol=1e-12)
+        assert np.allclose(d2[0, 0], s2 * np.cos(th * base), atol=1e-11)
+        # the symbols approximate the exact derivative to O(h^(npd-1))
+        assert s1 == pytest.approx(th / h, rel=5e-3 * k ** 6 / 1)
+    _ = x
+
+
+def test_field_consistency_free_droplet(pkg, ora):
+    """Without particles near the grid the impurity terms vanish and the
+    He mean field is symmetric under z -> -z for a centred droplet."""
+    p = pkg.workloads.make_params(24, 0.8, 4, pot=pkg.abi.HE4_POT_NULL)
+    psi = pkg.workloads.droplet_psi(p, 200)
+    r = np.full((3, 4), 1e6)  # outside the box: no deposit, zero force
+    v = np.zeros((3, 4))
+    o = ora.Oracle(p)
+    o.set_state(psi, r, v)
+    o.field()
+    assert np.all(o.get_field("denx") == 0) and np.all(o.get_field("uimp") == 0)
+    pot = o.get_field("pot4")
+    # grid points z_k = -zmax + k h: the reflection z -> -z maps k -> n - k
+    refl = np.roll(pot[::-1], 1, axis=0)
+    assert np.allclose(pot, refl, rtol=0, atol=1e-10 * np.abs(pot).max())
+    e = o.energy()
+    assert e["eHeX"] == 0.0 and e["ekinqx"] == 0.0
+    assert e["etot4"] < 0  # a bound droplet
+    o.close()
