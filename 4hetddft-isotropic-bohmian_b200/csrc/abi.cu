@@ -290,6 +290,7 @@ int he4_set_state(he4_handle *hh, const double *psi, const double *rimp, const d
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->have_state = 1;
   h->nsteps_done = 0;
+  h->field_valid = 0;
   return HE4_OK;
 }
 
@@ -313,6 +314,7 @@ static int sync_and_check(Handle *h) {
 int he4_potenimp(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
+  h->field_valid = 0;
   HE4_TRY(field_potenimp(h));
   return sync_and_check(h);
 }
@@ -320,6 +322,7 @@ int he4_potenimp(he4_handle *hh) {
 int he4_poten(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
+  h->field_valid = 0;
   HE4_TRY(field_poten(h));
   return sync_and_check(h);
 }
@@ -328,15 +331,14 @@ int he4_forceimp(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
   HE4_TRY(field_forceimp(h));
+  h->field_valid = 1;  // potenimp, poten, forceimp: the reference's sequence
   return sync_and_check(h);
 }
 
 int he4_field(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
-  HE4_TRY(field_potenimp(h));
-  HE4_TRY(field_poten(h));
-  HE4_TRY(field_forceimp(h));
+  HE4_TRY(field_all(h));
   return sync_and_check(h);
 }
 
@@ -432,6 +434,7 @@ int he4_energy(he4_handle *hh, he4_energies *e) {
     set_error("null energies");
     return HE4_E_ARG;
   }
+  if (!h->field_valid) HE4_TRY(field_all(h));  // energy() follows a field evaluation
   HE4_TRY(compute_energy(h, e));
   const double *v = &e->etot;
   if (!finite_all(v, 11)) {

@@ -138,6 +138,9 @@ struct Handle {
 
   int have_state = 0;
   int nsteps_done = 0;
+  // pot4, aimp and the other fields belong to the current psi and rimp
+  // (the field evaluation that DFT4He3d.f90:630-634 does before the loop)
+  int field_valid = 0;
   size_t red_len = 0;
 };
 
@@ -166,6 +169,8 @@ int setup_kernels(Handle *h);
 int field_potenimp(Handle *h);
 int field_poten(Handle *h);
 int field_forceimp(Handle *h);
+// potenimp + poten + forceimp; marks the fields valid
+int field_all(Handle *h);
 
 // dres: device array of 12 doubles: errHe, errimp, errvimp, then the 9 means
 int step_rk(Handle *h, double dt, double *dres);

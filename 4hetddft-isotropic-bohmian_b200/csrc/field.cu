@@ -56,7 +56,9 @@ __global__ void k_iron(const double *__restrict__ src, double *dst, double *sqrt
   if (i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1) {
     const size_t sy = g.nx, sz = (size_t)g.nx * g.ny;
     const double s6 = ((((src[t - 1] + src[t + 1]) + src[t - sy]) + src[t + sy]) + src[t - sz]) + src[t + sz];
-    v = (1.0 / 12.0) * s6 + 0.5 * src[t];
+    // separately rounded products (no FMA) so denx is bit-identical to the
+    // reference's arithmetic
+    v = __dadd_rn(__dmul_rn(1.0 / 12.0, s6), __dmul_rn(0.5, src[t]));
   } else {
     v = src[t];
   }

@@ -251,10 +251,12 @@ int compute_den(Handle *h) {
   return HE4_OK;
 }
 
-static int field_all(Handle *h) {
+int field_all(Handle *h) {
+  h->field_valid = 0;
   HE4_TRY(field_potenimp(h));
   HE4_TRY(field_poten(h));
   HE4_TRY(field_forceimp(h));
+  h->field_valid = 1;
   return HE4_OK;
 }
 
@@ -275,6 +277,7 @@ static void rot3(T *a) {  // (a0,a1,a2) <- (a2,a0,a1): physical shift of steprk.
 // dres: device array, [0..2] errors (zero for RK) and [3..11] means
 int step_rk(Handle *h, double dt, double *dres) {
   const Geo g = geo(h);
+  if (!h->field_valid) HE4_TRY(field_all(h));  // DFT4He3d.f90:630-634
   const double s2 = sqrt(2.0);
   const double arun[4] = {0.5, 1.0 - 1.0 / s2, 1.0 + 1.0 / s2, 1.0 / 6.0};
   const double brun[4] = {2.0, 1.0, 1.0, 2.0};
@@ -314,6 +317,7 @@ int step_rk(Handle *h, double dt, double *dres) {
 int step_pc(Handle *h, double dt, double *dres) {
   const Geo g = geo(h);
   const PsiArgs pa = psi_args(h, dt);
+  if (!h->field_valid) HE4_TRY(field_all(h));
   // predictor + modifier for psi
   {
     double2 *p3 = h->psiold[h->ioldp[2]];

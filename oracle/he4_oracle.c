@@ -661,6 +661,7 @@ struct ora_state {
   double *sto[7];
   cplx *fden, *wk1, *wk2, *wk3, *c1, *c2, *c3, *c4, *c5;
   int have_state, nsteps_done;
+  int field_valid; /* fields belong to the current psi/rimp (DFT4He3d.f90:630-634) */
 };
 
 static void *xalloc(size_t n) {
@@ -1029,6 +1030,7 @@ static void denpart(ora_state *s) {
 
 int ora_potenimp(ora_state *s) {
   if (!s || !s->have_state) return HE4_E_STATE;
+  s->field_valid = 0;
   denpart(s);
   fwd(s, s->denx, s->wk1);
 #pragma omp parallel for schedule(static)
@@ -1094,6 +1096,7 @@ static void term_alfa(ora_state *s) {
 /* poten (poten.f90:5-129) */
 int ora_poten(ora_state *s) {
   if (!s || !s->have_state) return HE4_E_STATE;
+  s->field_valid = 0;
   size_t N = s->N, H = s->H;
   const he4_params *p = &s->p;
   fwd(s, s->den, s->fden);
@@ -1200,6 +1203,7 @@ int ora_forceimp(ora_state *s) {
     s->fz[t] = (s->fz[t] + inv * (st[2][t] * hp - ps * st[5][t])) / m;
   }
   interpola3(s);
+  s->field_valid = 1; /* potenimp, poten, forceimp: the reference's sequence */
   return HE4_OK;
 }
 
@@ -1238,6 +1242,7 @@ int ora_set_state(ora_state *s, const double *psi, const double *rimp, const dou
   for (int i = 0; i < 2; i++) s->ioldh[i] = s->iolda[i] = i;
   s->have_state = 1;
   s->nsteps_done = 0;
+  s->field_valid = 0;
   return HE4_OK;
 }
 
@@ -1298,6 +1303,10 @@ static void set_den(ora_state *s) {
 /* steprk (steprk.f90:1-128) followed by the field evaluation */
 int ora_step_rk(ora_state *s, double dt, double means[9]) {
   if (!s || !s->have_state) return HE4_E_STATE;
+  if (!s->field_valid) { /* the first field of DFT4He3d.f90:630-634 */
+    int e0 = ora_field(s);
+    if (e0) return e0;
+  }
   size_t N = s->N;
   int np = s->p.n_par;
   size_t P3 = 3 * (size_t)np;
@@ -1358,6 +1367,10 @@ int ora_step_rk(ora_state *s, double dt, double means[9]) {
 /* steppc (steppc.f90:1-155) followed by the field evaluation */
 int ora_step_pc(ora_state *s, double dt, double err[3], double means[9]) {
   if (!s || !s->have_state) return HE4_E_STATE;
+  if (!s->field_valid) {
+    int e0 = ora_field(s);
+    if (e0) return e0;
+  }
   size_t N = s->N;
   int np = s->p.n_par;
   size_t P3 = 3 * (size_t)np;
@@ -1480,6 +1493,10 @@ int ora_run(ora_state *s, int32_t nsteps, double dt, double *err, double *means)
 
 int ora_energy(ora_state *s, he4_energies *E) {
   if (!s || !E || !s->have_state) return HE4_E_STATE;
+  if (!s->field_valid) { /* energy() follows a field evaluation */
+    int e0 = ora_field(s);
+    if (e0) return e0;
+  }
   size_t N = s->N;
   const he4_params *p = &s->p;
   deriv_c(s, 1, 0, s->psi, s->c1);

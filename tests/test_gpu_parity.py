@@ -2,8 +2,9 @@
 oracle on the same seeded inputs.
 
 Tolerances (FP64 everywhere):
-  * k-space kernels: pmod bit-identical; wcgk, kalfs 1e-14 and fvlj4 1e-11
-    relative to the largest value (different sin/cos/exp implementations);
+  * k-space kernels: pmod bit-identical; wcgk, kalfs 1e-14 and fvlj4 1e-8
+    relative to the largest value (different sin/cos/exp implementations,
+    amplified by the cancellation inside the reference's sinx11);
     Vq (single-precision values) within one FP32 ulp.
   * one field evaluation: every field within 1e-11 of its largest value.
   * energies after a field evaluation: 1e-10 relative per component.
@@ -49,7 +50,10 @@ def test_kspace_kernels(pkg, c1):
         assert np.array_equal(g.get_kernel("pmod"), o.get_kernel("pmod"))
         assert rel(g.get_kernel("wcgk"), o.get_kernel("wcgk")) < 1e-14
         assert rel(g.get_kernel("kalfs"), o.get_kernel("kalfs")) < 1e-14
-        assert rel(g.get_kernel("fvlj4"), o.get_kernel("fvlj4")) < 1e-11
+        # sinx11 (fforma.f90:96-100) subtracts two terms that agree to ~6
+        # digits at the largest |p|, so 1-ulp differences between libm's and
+        # CUDA's sin/cos become ~1e-9 relative there
+        assert rel(g.get_kernel("fvlj4"), o.get_kernel("fvlj4")) < 1e-8
         gv = g.get_kernel("vq")
         # both are single-precision numbers; at most one FP32 ulp apart
         ulp = np.spacing(np.abs(vq).astype(np.float32)).astype(np.float64)
