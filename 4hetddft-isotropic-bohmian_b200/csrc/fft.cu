@@ -20,6 +20,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "fft_reg.cuh"
 
 namespace he4 {
 
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_conv(ZArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// host side
+// twiddle tables
 // ---------------------------------------------------------------------------
 static int axis_init(AxisPlan &A, int n) {
   A.n = n;
@@ -381,6 +382,261 @@ static int axis_init(AxisPlan &A, int n) {
   return HE4_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// register-resident passes for power-of-two axes (16..256); see fft_reg.cuh
+// ---------------------------------------------------------------------------
+template <int N>
+struct RegShape;
+template <>
+struct RegShape<16> { static constexpr int N1 = 4; };
+template <>
+struct RegShape<32> { static constexpr int N1 = 4; };
+template <>
+struct RegShape<64> { static constexpr int N1 = 8; };
+template <>
+struct RegShape<128> { static constexpr int N1 = 8; };
+template <>
+struct RegShape<256> { static constexpr int N1 = 16; };
+
+static bool reg_ok(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256; }
+
+constexpr int kMaxOut = 6;
+struct ZOut {
+  double2 *out;
+  const double *kern;
+  double coef;
+  int dsym_axis;
+};
+struct ZGroup {
+  const double2 *in;
+  int nout;
+  ZOut o[kMaxOut];
+};
+
+struct YRegArgs {
+  PencilMap map;
+  long sf;
+  const double2 *tw;
+  double2 *buf[kMaxBatch];
+};
+
+struct ZRegArgs {
+  PencilMap map;
+  long sf;
+  int nx, ny;
+  const double *dsym;
+  const double2 *tw;
+  ZGroup g[kMaxBatch];
+};
+
+struct XRegArgs {
+  int nxh;
+  long nrow;
+  double scale;
+  const double2 *tw;
+  const double *rin[kMaxBatch];
+  double2 *cout[kMaxBatch];
+  const double2 *cin[kMaxBatch];
+  double *rout[kMaxBatch];
+};
+
+template <int N>
+__device__ __forceinline__ void load_tw_n(double2 *s_tw, const double2 *__restrict__ g_tw) {
+  for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = g_tw[t];
+}
+
+template <int N>
+static size_t smem_yz_reg() {
+  constexpr int N1 = RegShape<N>::N1, W = kThreads / N1;
+  return sizeof(double2) * ((size_t)N * W + N) + (sizeof(long) + 2 * sizeof(int)) * W;
+}
+template <int N>
+static size_t smem_x_reg() {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kThreads / N1;
+  return sizeof(double2) * ((size_t)P * N2 * (N1 + 1) + N);
+}
+
+// in-place transform of strided pencils (y pass, or z without multiply)
+template <int N, bool INV>
+__global__ void __launch_bounds__(kThreads) k_yz_reg(YRegArgs a) {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kThreads / N1;
+  extern __shared__ double2 smem[];
+  double2 *S = smem, *tw = smem + N * W;
+  long *offs = reinterpret_cast<long *>(tw + N);
+  load_tw_n<N>(tw, a.tw);
+  if (threadIdx.x < W) {
+    int kx, o;
+    offs[threadIdx.x] = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
+  }
+  __syncthreads();
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  const long off = offs[w];
+  double2 *data = a.buf[blockIdx.y];
+  double2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? data[off + (j1 + N1 * j2) * a.sf] : make_double2(0.0, 0.0);
+  regfft::LayoutYZ lay{W, w};
+  regfft::fwd2<N, N1, INV>(v, S, lay, j1, tw);
+  if (off < 0) return;
+#pragma unroll
+  for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) data[off + ((j1 + N1 * c) + N2 * k1) * a.sf] = v[c * N1 + k1];
+}
+
+// z pass: one input per group, FFT_z once, then for each output
+// IFFT_z(coef * K(k) [* i D(k)] * X)
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_zconv_reg(ZRegArgs a) {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kThreads / N1;
+  extern __shared__ double2 smem[];
+  double2 *S = smem, *tw = smem + N * W;
+  long *offs = reinterpret_cast<long *>(tw + N);
+  int *kxs = reinterpret_cast<int *>(offs + W);
+  int *kys = kxs + W;
+  load_tw_n<N>(tw, a.tw);
+  if (threadIdx.x < W) {
+    int kx = 0, o = 0;
+    offs[threadIdx.x] = pencil_offset(a.map, (long)blockIdx.y * W + threadIdx.x, &kx, &o);
+    kxs[threadIdx.x] = kx;
+    kys[threadIdx.x] = o;
+  }
+  __syncthreads();
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  const long off = offs[w];
+  const ZGroup &G = a.g[blockIdx.x];
+  double2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? G.in[off + (j1 + N1 * j2) * a.sf] : make_double2(0.0, 0.0);
+  regfft::LayoutYZ lay{W, w};
+  regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
+  const double dx = (off >= 0) ? a.dsym[kxs[w]] : 0.0;
+  const double dy = (off >= 0) ? a.dsym[a.nx + kys[w]] : 0.0;
+  for (int o = 0; o < G.nout; o++) {
+    const ZOut Z = G.o[o];
+    double2 u[N2];
+#pragma unroll
+    for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) {
+        const int k = (j1 + N1 * c) + N2 * k1;
+        double cf = Z.coef;
+        if (Z.kern && off >= 0) cf *= __ldg(Z.kern + off + k * a.sf);
+        double2 x = cscale(v[c * N1 + k1], cf);
+        if (Z.dsym_axis >= 0) {
+          const double ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
+          x = make_double2(-x.y * ds, x.x * ds);
+        }
+        u[c * N1 + k1] = x;
+      }
+    regfft::bwd2<N, N1, true>(u, S, lay, j1, tw);
+    if (off >= 0) {
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) Z.out[off + (j1 + N1 * n2) * a.sf] = u[n2];
+    }
+  }
+}
+
+// x pass R2C: two real rows per complex pencil, Hermitian split
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_xr2c_reg(XRegArgs a) {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kThreads / N1, SP = N2 * (N1 + 1);
+  extern __shared__ double2 smem[];
+  double2 *S = smem, *tw = smem + P * SP;
+  load_tw_n<N>(tw, a.tw);
+  __syncthreads();
+  const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
+  const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
+  const double *in = a.rin[blockIdx.y];
+  double2 *out = a.cout[blockIdx.y];
+  double2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) {
+    const int x = j1 + N1 * j2;
+    v[j2] = make_double2((ra < a.nrow) ? in[ra * N + x] : 0.0, (rb < a.nrow) ? in[rb * N + x] : 0.0);
+  }
+  regfft::LayoutX lay{p * SP};
+  regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
+  double2 *Sp = S + p * SP;
+#pragma unroll
+  for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) Sp[(j1 + N1 * c) + N2 * k1] = v[c * N1 + k1];
+  __syncthreads();
+  for (int k = j1; k <= N / 2; k += N1) {
+    const double2 zk = Sp[k];
+    const double2 zm = cconj(Sp[(N - k) & (N - 1)]);
+    const double2 A = cscale(cadd(zk, zm), 0.5);
+    const double2 d = cscale(csub(zk, zm), 0.5);
+    if (ra < a.nrow) out[ra * a.nxh + k] = A;
+    if (rb < a.nrow) out[rb * a.nxh + k] = make_double2(d.y, -d.x);
+  }
+}
+
+// x pass C2R: Hermitian extension of two half spectra, inverse, two rows
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_xc2r_reg(XRegArgs a) {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kThreads / N1, SP = N2 * (N1 + 1);
+  extern __shared__ double2 smem[];
+  double2 *S = smem, *tw = smem + P * SP;
+  load_tw_n<N>(tw, a.tw);
+  const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
+  const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
+  const double2 *in = a.cin[blockIdx.y];
+  double *out = a.rout[blockIdx.y];
+  double2 *Sp = S + p * SP;
+  for (int k = j1; k < a.nxh; k += N1) {
+    double2 X = (ra < a.nrow) ? in[ra * a.nxh + k] : make_double2(0.0, 0.0);
+    double2 Y = (rb < a.nrow) ? in[rb * a.nxh + k] : make_double2(0.0, 0.0);
+    if (k == 0 || 2 * k == N) {  // DC / Nyquist of a real transform: drop Im
+      X.y = 0.0;
+      Y.y = 0.0;
+    }
+    Sp[k] = make_double2(X.x - Y.y, X.y + Y.x);
+    if (k > 0 && N - k >= a.nxh) Sp[N - k] = make_double2(X.x + Y.y, Y.x - X.y);
+  }
+  __syncthreads();
+  double2 v[N2];
+#pragma unroll
+  for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) v[c * N1 + k1] = Sp[(j1 + N1 * c) + N2 * k1];
+  __syncthreads();
+  regfft::LayoutX lay{p * SP};
+  regfft::bwd2<N, N1, true>(v, S, lay, j1, tw);
+  const double sc = a.scale;
+#pragma unroll
+  for (int n2 = 0; n2 < N2; n2++) {
+    const int x = j1 + N1 * n2;
+    if (ra < a.nrow) out[ra * N + x] = v[n2].x * sc;
+    if (rb < a.nrow) out[rb * N + x] = v[n2].y * sc;
+  }
+}
+
+template <int N>
+static int reg_attrs() {
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N>()));
+  return HE4_OK;
+}
+
+// run the statement with NN = n (n one of the register-path lengths)
+#define HE4_REG_SWITCH(n, ...)                                  \
+  switch (n) {                                                  \
+    case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
+    case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
+    case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
+    case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
+    default: { constexpr int NN = 256; __VA_ARGS__; } break;    \
+  }
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
 static int tile_width(int n) {
   int w = 2048 / n;
   w = (w / 8) * 8;
@@ -408,6 +664,9 @@ int fft_plan_init(FftPlan &P, int nx, int ny, int nz) {
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(ny, P.wy)));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(ny, P.wy)));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(nz, P.wz)));
+  const int ns[3] = {nx, ny, nz};
+  for (int n : ns)
+    if (reg_ok(n)) HE4_REG_SWITCH(n, HE4_TRY(reg_attrs<NN>()));
   return HE4_OK;
 }
 
@@ -418,77 +677,179 @@ void fft_plan_free(FftPlan &P) {
   P.ax.tw = P.ay.tw = P.az.tw = nullptr;
 }
 
-int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out) {
+static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *cout, double2 *const *cin,
+                  double *const *rout, bool inverse) {
   const FftPlan &P = h->fft;
+  const long nrow = (long)P.ny * P.nz;
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
-    int nb = std::min(kMaxBatch, n - b0);
-    XArgs a{};
-    a.ax = P.ax;
-    a.nxh = P.nxh;
-    a.P = P.px;
-    a.nrow = (long)P.ny * P.nz;
-    a.scale = 1.0;
-    for (int i = 0; i < nb; i++) {
-      a.rin[i] = in[b0 + i];
-      a.cout[i] = out[b0 + i];
+    const int nb = std::min(kMaxBatch, n - b0);
+    if (reg_ok(P.nx)) {
+      XRegArgs a{};
+      a.nxh = P.nxh;
+      a.nrow = nrow;
+      a.scale = 1.0;
+      a.tw = P.ax.tw;
+      for (int i = 0; i < nb; i++) {
+        if (inverse) {
+          a.cin[i] = cin[b0 + i];
+          a.rout[i] = rout[b0 + i];
+        } else {
+          a.rin[i] = rin[b0 + i];
+          a.cout[i] = cout[b0 + i];
+        }
+      }
+      HE4_REG_SWITCH(P.nx, {
+        constexpr int Pp = kThreads / RegShape<NN>::N1;
+        dim3 grid((unsigned)((nrow + 2 * Pp - 1) / (2 * Pp)), nb);
+        if (inverse)
+          k_xc2r_reg<NN><<<grid, kThreads, smem_x_reg<NN>(), h->stream>>>(a);
+        else
+          k_xr2c_reg<NN><<<grid, kThreads, smem_x_reg<NN>(), h->stream>>>(a);
+      });
+    } else {
+      XArgs a{};
+      a.ax = P.ax;
+      a.nxh = P.nxh;
+      a.P = P.px;
+      a.nrow = nrow;
+      a.scale = 1.0;
+      for (int i = 0; i < nb; i++) {
+        if (inverse) {
+          a.cin[i] = cin[b0 + i];
+          a.rout[i] = rout[b0 + i];
+        } else {
+          a.rin[i] = rin[b0 + i];
+          a.cout[i] = cout[b0 + i];
+        }
+      }
+      dim3 grid((unsigned)((nrow + 2 * P.px - 1) / (2 * P.px)), nb);
+      if (inverse)
+        k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+      else
+        k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
     }
-    dim3 grid((unsigned)((a.nrow + 2 * P.px - 1) / (2 * P.px)), nb);
-    k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
     HE4_LAUNCHED(h);
   }
-  double2 *bufs[64];
-  for (int i = 0; i < n; i++) bufs[i] = out[i];
-  HE4_TRY(fft_y(h, n, bufs, false));
   return HE4_OK;
 }
 
-int fft_y(Handle *h, int n, double2 *const *buf, bool inverse) {
+// in-place complex transform of every pencil along y (axis 1) or z (axis 2)
+static int strided_pass(Handle *h, int n, double2 *const *buf, int axis, bool inverse) {
   const FftPlan &P = h->fft;
+  const int len = (axis == 1) ? P.ny : P.nz;
+  const AxisPlan &A = (axis == 1) ? P.ay : P.az;
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
-    int nb = std::min(kMaxBatch, n - b0);
-    YArgs a{};
-    a.ay = P.ay;
-    a.map.nxh = P.nxh;
-    a.map.nother = P.nz;
-    a.map.W = P.wy;
-    a.map.so = (long)P.ny * P.nxh;
-    a.sf = P.nxh;
-    for (int i = 0; i < nb; i++) a.buf[i] = buf[b0 + i];
-    long total = (long)P.nxh * P.nz;
-    dim3 grid((unsigned)((total + P.wy - 1) / P.wy), nb);
-    if (inverse)
-      k_fft_y<true><<<grid, kThreads, smem_yz(P.ny, P.wy), h->stream>>>(a);
-    else
-      k_fft_y<false><<<grid, kThreads, smem_yz(P.ny, P.wy), h->stream>>>(a);
-    HE4_LAUNCHED(h);
+    const int nb = std::min(kMaxBatch, n - b0);
+    PencilMap map;
+    map.nxh = P.nxh;
+    map.nother = (axis == 1) ? P.nz : P.ny;
+    map.so = (axis == 1) ? (long)P.ny * P.nxh : P.nxh;
+    const long sf = (axis == 1) ? (long)P.nxh : (long)P.ny * P.nxh;
+    const long total = (long)P.nxh * map.nother;
+    if (reg_ok(len)) {
+      YRegArgs a{};
+      a.sf = sf;
+      a.tw = A.tw;
+      for (int i = 0; i < nb; i++) a.buf[i] = buf[b0 + i];
+      HE4_REG_SWITCH(len, {
+        constexpr int W = kThreads / RegShape<NN>::N1;
+        map.W = W;
+        a.map = map;
+        dim3 grid((unsigned)((total + W - 1) / W), nb);
+        if (inverse)
+          k_yz_reg<NN, true><<<grid, kThreads, smem_yz_reg<NN>(), h->stream>>>(a);
+        else
+          k_yz_reg<NN, false><<<grid, kThreads, smem_yz_reg<NN>(), h->stream>>>(a);
+      });
+      HE4_LAUNCHED(h);
+    } else if (axis == 1) {
+      YArgs a{};
+      a.ay = P.ay;
+      map.W = P.wy;
+      a.map = map;
+      a.sf = sf;
+      for (int i = 0; i < nb; i++) a.buf[i] = buf[b0 + i];
+      dim3 grid((unsigned)((total + P.wy - 1) / P.wy), nb);
+      if (inverse)
+        k_fft_y<true><<<grid, kThreads, smem_yz(P.ny, P.wy), h->stream>>>(a);
+      else
+        k_fft_y<false><<<grid, kThreads, smem_yz(P.ny, P.wy), h->stream>>>(a);
+      HE4_LAUNCHED(h);
+    } else {
+      for (int i = 0; i < nb; i++) {
+        ZOp op{buf[b0 + i], buf[b0 + i], nullptr, 1.0, -1, inverse ? 2 : 1};
+        HE4_TRY(fft_z_conv(h, 1, &op));
+      }
+    }
   }
+  return HE4_OK;
+}
+
+int fft_y(Handle *h, int n, double2 *const *buf, bool inverse) { return strided_pass(h, n, buf, 1, inverse); }
+
+int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out) {
+  HE4_TRY(x_pass(h, n, in, out, nullptr, nullptr, false));
+  HE4_TRY(fft_y(h, n, out, false));
   return HE4_OK;
 }
 
 int fft_c2r(Handle *h, int n, double2 *const *in, double *const *out) {
-  const FftPlan &P = h->fft;
   HE4_TRY(fft_y(h, n, in, true));
-  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
-    int nb = std::min(kMaxBatch, n - b0);
-    XArgs a{};
-    a.ax = P.ax;
-    a.nxh = P.nxh;
-    a.P = P.px;
-    a.nrow = (long)P.ny * P.nz;
-    a.scale = 1.0;
-    for (int i = 0; i < nb; i++) {
-      a.cin[i] = in[b0 + i];
-      a.rout[i] = out[b0 + i];
-    }
-    dim3 grid((unsigned)((a.nrow + 2 * P.px - 1) / (2 * P.px)), nb);
-    k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
-    HE4_LAUNCHED(h);
-  }
+  HE4_TRY(x_pass(h, n, nullptr, nullptr, in, out, true));
   return HE4_OK;
 }
 
 int fft_z_conv(Handle *h, int n, const ZOp *ops) {
   const FftPlan &P = h->fft;
+  if (n <= 0) return HE4_OK;
+  const bool plain = ops[0].mode != 0;
+  if (reg_ok(P.nz) && !plain) {
+    // group consecutive operations that read the same input
+    ZGroup groups[64];
+    int ng = 0;
+    for (int i = 0; i < n; i++) {
+      if (ng == 0 || groups[ng - 1].in != ops[i].in || groups[ng - 1].nout == kMaxOut) {
+        groups[ng].in = ops[i].in;
+        groups[ng].nout = 0;
+        ng++;
+      }
+      ZGroup &g = groups[ng - 1];
+      g.o[g.nout++] = ZOut{ops[i].out, ops[i].kern, ops[i].coef, ops[i].dsym_axis};
+    }
+    for (int g0 = 0; g0 < ng; g0 += kMaxBatch) {
+      const int nb = std::min(kMaxBatch, ng - g0);
+      ZRegArgs a{};
+      a.map.nxh = P.nxh;
+      a.map.nother = P.ny;
+      a.map.so = P.nxh;
+      a.sf = (long)P.ny * P.nxh;
+      a.nx = P.nx;
+      a.ny = P.ny;
+      a.dsym = h->dsym;
+      a.tw = P.az.tw;
+      for (int i = 0; i < nb; i++) a.g[i] = groups[g0 + i];
+      const long total = (long)P.nxh * P.ny;
+      HE4_REG_SWITCH(P.nz, {
+        constexpr int W = kThreads / RegShape<NN>::N1;
+        a.map.W = W;
+        dim3 grid(nb, (unsigned)((total + W - 1) / W));
+        k_zconv_reg<NN><<<grid, kThreads, smem_yz_reg<NN>(), h->stream>>>(a);
+      });
+      HE4_LAUNCHED(h);
+    }
+    return HE4_OK;
+  }
+  if (reg_ok(P.nz) && plain) {
+    for (int i = 0; i < n; i++) {
+      double2 *b[1] = {ops[i].out};
+      if (ops[i].out != ops[i].in) {
+        set_error("plain z transforms are in place");
+        return HE4_E_ARG;
+      }
+      HE4_TRY(strided_pass(h, 1, b, 2, ops[i].mode == 2));
+    }
+    return HE4_OK;
+  }
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
     int nb = std::min(kMaxBatch, n - b0);
     ZArgs a{};
@@ -517,24 +878,11 @@ int fft_z_only(Handle *h, double2 *buf, bool inverse) {
 }
 
 int fft_x_only(Handle *h, const double *rin, double2 *cout, const double2 *cin, double *rout, bool inverse) {
-  const FftPlan &P = h->fft;
-  XArgs a{};
-  a.ax = P.ax;
-  a.nxh = P.nxh;
-  a.P = P.px;
-  a.nrow = (long)P.ny * P.nz;
-  a.scale = 1.0;
-  a.rin[0] = rin;
-  a.cout[0] = cout;
-  a.cin[0] = cin;
-  a.rout[0] = rout;
-  dim3 grid((unsigned)((a.nrow + 2 * P.px - 1) / (2 * P.px)), 1);
-  if (inverse)
-    k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
-  else
-    k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
-  HE4_LAUNCHED(h);
-  return HE4_OK;
+  const double *ri[1] = {rin};
+  double2 *co[1] = {cout};
+  double2 *ci[1] = {const_cast<double2 *>(cin)};
+  double *ro[1] = {rout};
+  return x_pass(h, 1, ri, co, ci, ro, inverse);
 }
 
 }  // namespace he4
