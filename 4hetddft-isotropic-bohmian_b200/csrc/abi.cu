@@ -444,6 +444,16 @@ int he4_energy(he4_handle *hh, he4_energies *e) {
   return HE4_OK;
 }
 
+int he4_diagnostics(he4_handle *hh, int32_t n4, double out[4]) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  if (!out || n4 <= 0) {
+    set_error("he4_diagnostics needs an output array and n4 > 0");
+    return HE4_E_ARG;
+  }
+  return compute_diagnostics(h, n4, out);
+}
+
 int he4_get_field(he4_handle *hh, int32_t which, double *out) {
   HANDLE_OR_FAIL(hh);
   if (!out) {

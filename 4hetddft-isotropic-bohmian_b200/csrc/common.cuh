@@ -176,6 +176,7 @@ int field_all(Handle *h);
 int step_rk(Handle *h, double dt, double *dres);
 int step_pc(Handle *h, double dt, double *dres);
 int compute_energy(Handle *h, he4_energies *e);
+int compute_diagnostics(Handle *h, int n4, double *host_out);
 int compute_den(Handle *h);
 int particle_means(Handle *h, double *means);
 

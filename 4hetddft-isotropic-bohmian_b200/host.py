@@ -50,6 +50,7 @@ def load_library():
     L.he4_run.argtypes = [vp, i32, C.c_double, dp, dp]
     L.he4_energy.argtypes = [vp, vp]
     L.he4_get_field.argtypes = [vp, i32, dp]
+    L.he4_diagnostics.argtypes = [vp, i32, dp]
     L.he4_get_kernel.argtypes = [vp, i32, dp]
     L.he4_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.he4_launch_count.argtypes = [vp]
@@ -158,6 +159,12 @@ class He4Step:
         E = abi.He4Energies()
         _check(load_library().he4_energy(self._h, C.byref(E)), "he4_energy")
         return E.as_dict()
+
+    def diagnostics(self, n4):
+        """(atom number, xcm, ycm, zcm) of the current density."""
+        out = np.zeros(4)
+        _check(load_library().he4_diagnostics(self._h, n4, _dp(out)), "he4_diagnostics")
+        return out
 
     def get_field(self, name):
         out = np.zeros(self.shape)

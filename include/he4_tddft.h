@@ -144,6 +144,11 @@ int he4_run(he4_handle *h, int32_t nsteps, double deltat, double *err,
 /* energy() (energy.f90:12-129) evaluated on the current fields. */
 int he4_energy(he4_handle *h, he4_energies *e);
 
+/* Diagnostics of the pener block reduced on the device: out[0] = He atom
+ * number sum(den)*dxyz (DFT4He3d.f90:885-886), out[1..3] = centre of mass
+ * of den (r_cm.f90:23-58, divided by n4 as r_cm does). */
+int he4_diagnostics(he4_handle *h, int32_t n4, double out[4]);
+
 /* Copy-out of a real grid field ([nz][ny][nx]) or a half-spectrum kernel. */
 int he4_get_field(he4_handle *h, int32_t which, double *out);
 int he4_get_kernel(he4_handle *h, int32_t which, double *out);

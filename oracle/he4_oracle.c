@@ -1543,6 +1543,23 @@ int ora_energy(ora_state *s, he4_energies *E) {
   return HE4_OK;
 }
 
+/* atom number sum(den)*dxyz (DFT4He3d.f90:885-886) and centre of mass
+ * (r_cm.f90:40-56) */
+int ora_diagnostics(ora_state *s, int32_t n4, double out[4]) {
+  if (!s || !out || n4 <= 0 || !s->have_state) return HE4_E_ARG;
+  int nx = s->nx, ny = s->ny;
+  double s0, sx, sy, sz;
+  DET_SUM(s0, s->N, s->den[i]);
+  DET_SUM(sx, s->N, s->den[i] * s->x[i % nx]);
+  DET_SUM(sy, s->N, s->den[i] * s->y[(i / nx) % ny]);
+  DET_SUM(sz, s->N, s->den[i] * s->z[i / ((size_t)nx * ny)]);
+  out[0] = s0 * s->dxyz;
+  out[1] = sx * s->dxyz / n4;
+  out[2] = sy * s->dxyz / n4;
+  out[3] = sz * s->dxyz / n4;
+  return HE4_OK;
+}
+
 int ora_get_field(ora_state *s, int32_t which, double *out) {
   if (!s || !out) return HE4_E_ARG;
   const double *src = NULL;

@@ -35,6 +35,7 @@ int ora_step_pc(ora_state *s, double deltat, double err[3], double means[9]);
 int ora_run(ora_state *s, int32_t nsteps, double deltat, double *err,
             double *means);
 int ora_energy(ora_state *s, he4_energies *e);
+int ora_diagnostics(ora_state *s, int32_t n4, double out[4]);
 int ora_get_field(ora_state *s, int32_t which, double *out);
 int ora_get_kernel(ora_state *s, int32_t which, double *out);
 void ora_set_threads(int n);

@@ -49,6 +49,7 @@ def _declare(L):
     L.ora_step_pc.argtypes = [vp, C.c_double, dp, dp]
     L.ora_run.argtypes = [vp, i32, C.c_double, dp, dp]
     L.ora_energy.argtypes = [vp, vp]
+    L.ora_diagnostics.argtypes = [vp, i32, dp]
     L.ora_get_field.argtypes = [vp, i32, dp]
     L.ora_get_kernel.argtypes = [vp, i32, dp]
     L.ora_set_threads.argtypes = [C.c_int]
@@ -185,6 +186,11 @@ class Oracle:
         E = from_abi.He4Energies()
         _check(lib().ora_energy(self._h, C.byref(E)), "energy")
         return E.as_dict()
+
+    def diagnostics(self, n4):
+        out = np.zeros(4)
+        _check(lib().ora_diagnostics(self._h, n4, _dp(out)), "diagnostics")
+        return out
 
     def get_field(self, name):
         import sys

@@ -179,6 +179,23 @@ def test_field_parity_variants(pkg, ora, variant):
     o.close()
 
 
+def test_diagnostics_parity(pkg, c1):
+    """Atom number and centre of mass reduced on the device (DFT4He3d.f90:885,
+    r_cm.f90) against the oracle, after a few steps."""
+    p, psi, r, v, o, vq = c1
+    dt = pkg.workloads.deltat_fs(1.0)
+    o.set_state(psi, r, v)
+    o.run(5, dt)
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        d0 = g.diagnostics(300)
+        assert d0[0] == pytest.approx(np.sum(np.abs(psi) ** 2) * (2 * p.xmax / p.nx) ** 3, rel=1e-13)
+        g.run(5, dt)
+        dg, do = g.diagnostics(300), o.diagnostics(300)
+        assert abs(dg[0] - do[0]) <= 1e-12 * do[0]
+        assert np.allclose(dg[1:], do[1:], rtol=1e-9, atol=1e-12)
+
+
 def test_launch_count_and_errors(pkg, c1):
     p, psi, r, v, o, vq = c1
     with pkg.He4Step(p) as g:
