@@ -1,8 +1,21 @@
 // diag.cu -- device-side diagnostics of the pener blocks: the He atom number
 // sum(den)*dxyz (DFT4He3d.f90:885-886) and the centre of mass of the density
 // (r_cm.f90:23-58), reduced on the GPU so no field has to be copied out.
+//
+// Two entry points share the kernels: he4_diagnostics works on a handle and
+// takes its per-plane partial sums from the handle's reduction workspace;
+// he4_diagnostics_noalloc works on caller-owned device arrays and takes them
+// from the fixed array below, so it allocates nothing.
+#include <mutex>
+
 #include "common.cuh"
 #include "reduce.cuh"
+
+// Scratch of he4_diagnostics_noalloc: four partial sums per z plane.  It is
+// part of the library image, so every GPU that loads the library holds these
+// 128 KiB until the process exits.
+#define HE4_DIAG_NOALLOC_MAX_NZ 4096
+static __device__ __align__(256) double g_diag_noalloc_part[4 * HE4_DIAG_NOALLOC_MAX_NZ];
 
 namespace he4 {
 
@@ -81,6 +94,34 @@ static int launch_diag(const double *den, const DiagArgs &a, double dxyz, double
   return HE4_OK;
 }
 
+// Device address of g_diag_noalloc_part, looked up once per device (with that
+// device current) the first time he4_diagnostics_noalloc runs on it.  In host
+// code the symbol is only a stand-in; kernels must be given this address.
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+static int noalloc_scratch(double **out) {
+  int dev = -1;
+  HE4_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device ordinal %d out of range", dev);
+    return HE4_E_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_diag_noalloc_part);
+    if (e != cudaSuccess || !p) {
+      set_error("cudaGetSymbolAddress of the diagnostics scratch: %s", cudaGetErrorString(e));
+      return HE4_E_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<double *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return HE4_OK;
+}
+
 int compute_diagnostics(Handle *h, int n4, double *host_out) {
   const DiagArgs a = diag_args(h->nx, h->ny, h->nz, h->p.xmax, h->p.ymax, h->p.zmax);
   // scratch: the reduction workspace (8 * nblocks >= 4 * nz doubles)
@@ -92,3 +133,25 @@ int compute_diagnostics(Handle *h, int n4, double *host_out) {
 }
 
 }  // namespace he4
+
+extern "C" int he4_diagnostics_noalloc(const double *den, int32_t nx, int32_t ny, int32_t nz, double xmax,
+                                       double ymax, double zmax, int32_t n4, double *out, void *stream) {
+  using namespace he4;
+  if (!den || !out || nx <= 0 || ny <= 0 || nz <= 0 || n4 <= 0 || !(xmax > 0) || !(ymax > 0) || !(zmax > 0)) {
+    set_error("he4_diagnostics_noalloc: null array or non-positive size");
+    return HE4_E_ARG;
+  }
+  if (nz > HE4_DIAG_NOALLOC_MAX_NZ) {
+    set_error("he4_diagnostics_noalloc: nz=%d exceeds the fixed scratch of %d planes", nz, HE4_DIAG_NOALLOC_MAX_NZ);
+    return HE4_E_ARG;
+  }
+  if ((int64_t)nx * ny > (int64_t)1 << 30) {
+    set_error("he4_diagnostics_noalloc: nx*ny=%lld too large", (long long)nx * ny);
+    return HE4_E_ARG;
+  }
+  double *part = nullptr;
+  HE4_TRY(noalloc_scratch(&part));
+  const DiagArgs a = diag_args(nx, ny, nz, xmax, ymax, zmax);
+  const double dxyz = a.hx * a.hy * a.hz;
+  return launch_diag(den, a, dxyz, (double)n4, part, out, static_cast<cudaStream_t>(stream), nullptr);
+}

@@ -149,6 +149,25 @@ int he4_energy(he4_handle *h, he4_energies *e);
  * of den (r_cm.f90:23-58, divided by n4 as r_cm does). */
 int he4_diagnostics(he4_handle *h, int32_t n4, double out[4]);
 
+/* he4_diagnostics without a handle and without any allocation.  It has no
+ * counterpart in the reference; it exists for callers that cannot call
+ * cudaMalloc: hosts whose device memory belongs to another allocator (a
+ * framework's memory pool, a Fortran runtime's device arrays) and that may
+ * not add raw cudaMalloc/cudaFree calls, cudaFree being a device-wide
+ * synchronisation.  den is a device array [nz][ny][nx]; out is a device
+ * array of 4 doubles receiving what he4_diagnostics returns; stream is a
+ * cudaStream_t (NULL: the legacy default stream); the call is asynchronous
+ * on that stream.  Its scratch is a fixed 128 KiB array inside the library
+ * (four partial sums per z plane), so nz may not exceed 4096: larger grids
+ * return HE4_E_ARG.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress, with the device current); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that may overlap on the GPU (other streams, other threads) race and
+ * must be serialised by the caller. */
+int he4_diagnostics_noalloc(const double *den, int32_t nx, int32_t ny, int32_t nz,
+                            double xmax, double ymax, double zmax, int32_t n4,
+                            double *out, void *stream);
+
 /* Copy-out of a real grid field ([nz][ny][nx]) or a half-spectrum kernel. */
 int he4_get_field(he4_handle *h, int32_t which, double *out);
 int he4_get_kernel(he4_handle *h, int32_t which, double *out);
