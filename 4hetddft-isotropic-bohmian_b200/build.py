@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhe4b200.so")
-SOURCES = ["abi.cu", "fft.cu", "setup.cu", "field.cu", "step.cu", "energy.cu", "diag.cu"]
+SOURCES = ["abi.cu", "fft.cu", "setup.cu", "field.cu", "impurity.cu", "step.cu", "energy.cu", "diag.cu"]
 HEADERS = ["common.cuh", "stencil.cuh", "reduce.cuh", "fft_reg.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -55,7 +55,8 @@ def build(force=False, verbose=False, extra=()):
     if failed:
         raise RuntimeError("nvcc failed for " + ", ".join(failed))
     tmp = LIB + ".tmp"
-    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart"]
+    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart",
+           "-Xlinker", "--no-undefined"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

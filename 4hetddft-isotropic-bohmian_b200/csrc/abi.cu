@@ -93,7 +93,7 @@ static void free_all(Handle *h) {
                   h->dyden, h->dzden, h->penalty, h->corr, h->denx, h->psix, h->hpsix, h->uimp, h->fx, h->fy,
                   h->fz, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], h->counts, h->rimp, h->vimp, h->aimp,
                   h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
-                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal};
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->box};
   for (void *p : ptrs) cudaFree(p);
   for (int i = 0; i < 8; i++) cudaFree(h->spec[i]);
   if (h->hscal) cudaFreeHost(h->hscal);
@@ -155,6 +155,7 @@ static int create(const he4_params *pin, Handle *h) {
                         &h->rtmp[0], &h->rtmp[1], &h->rtmp[2], &h->rtmp[3]};
   for (double **f : rfields) HE4_TRY(dalloc(f, N));
   HE4_TRY(dalloc(&h->counts, N));
+  HE4_TRY(dalloc(&h->box, 1));
   for (int i = 0; i < 4; i++) HE4_TRY(dalloc(&h->spec[i], H));
   double **pfields[] = {&h->rimp, &h->vimp, &h->aimp, &h->rimpold[0], &h->rimpold[1], &h->rimpold[2],
                         &h->vimpold[0], &h->vimpold[1], &h->vimpold[2], &h->aimpold[0], &h->aimpold[1],
@@ -170,6 +171,8 @@ static int create(const he4_params *pin, Handle *h) {
   for (double2 **f : cfields) HE4_CUDA_TRY(cudaMemsetAsync(*f, 0, sizeof(double2) * N, h->stream));
   for (double **f : rfields) HE4_CUDA_TRY(cudaMemsetAsync(*f, 0, sizeof(double) * N, h->stream));
   for (double **f : pfields) HE4_CUDA_TRY(cudaMemsetAsync(*f, 0, sizeof(double) * P3, h->stream));
+  HE4_CUDA_TRY(cudaMemsetAsync(h->counts, 0, sizeof(unsigned int) * N, h->stream));
+  HE4_TRY(impurity_reset_box(h));
   he4_params with_table = p;
   with_table.vq_table = pin->vq_table;
   h->p = with_table;
@@ -560,6 +563,17 @@ static int launch_bench(Handle *h, int which) {
     }
     case 2: return fft_x_only(h, h->rtmp[0], h->spec[1], nullptr, nullptr, false);
     case 3: return fft_x_only(h, nullptr, nullptr, h->spec[1], h->rtmp[0], true);
+    case 4: return fft_z_only(h, h->spec[1], false);
+    case 5: {
+      ZOp op{h->spec[0], h->spec[1], nullptr, h->renor, -1};
+      return fft_z_conv(h, 1, &op);
+    }
+    case 6: {
+      ZOp ops[3] = {{h->spec[0], h->spec[1], h->wcgk, h->renor, -1},
+                    {h->spec[0], h->spec[2], h->fvlj4, h->renor, -1},
+                    {h->spec[0], h->spec[3], h->kalfs, h->renor, -1}};
+      return fft_z_conv(h, 3, ops);
+    }
     default: set_error("unknown kernel id %d", which); return HE4_E_ARG;
   }
 }
@@ -571,11 +585,13 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
     set_error("invalid arguments");
     return HE4_E_ARG;
   }
-  static const char *names[4] = {"k_fft_z_conv", "k_fft_y", "k_fft_x_r2c", "k_fft_x_c2r"};
+  static const char *names[7] = {"k_fft_z_conv",  "k_fft_y",           "k_fft_x_r2c", "k_fft_x_c2r",
+                                 "k_fft_z_plain", "k_fft_z_conv_nokern", "k_fft_z_conv_3out"};
   const double H = (double)h->H, N = (double)h->N;
   // algorithmic bytes: read input once, write output once (+ the real kernel)
-  const double bytes[4] = {16 * H + 8 * H + 16 * H, 2 * 16 * H, 8 * N + 16 * H, 16 * H + 8 * N};
-  if (which < 0 || which > 3) {
+  const double bytes[7] = {16 * H + 8 * H + 16 * H, 2 * 16 * H, 8 * N + 16 * H, 16 * H + 8 * N,
+                           2 * 16 * H, 2 * 16 * H, 16 * H + 3 * (8 * H + 16 * H)};
+  if (which < 0 || which > 6) {
     set_error("unknown kernel id %d", which);
     return HE4_E_ARG;
   }

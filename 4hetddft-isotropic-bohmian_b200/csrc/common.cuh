@@ -93,6 +93,16 @@ int fd_weights(int npd, int order, double *w);
 
 struct ZOp;  // z-pass operation (fft.cu)
 
+// support box of the impurity fields (impurity.cu): inclusive cell ranges
+struct Box {
+  int lo[3], hi[3];
+  int full;   // the whole grid (the box would wrap or reach a face)
+  int empty;  // no particle inside the grid
+};
+struct BoxPair {
+  Box cur, prev;
+};
+
 // ---------------------------------------------------------------------------
 // the handle
 // ---------------------------------------------------------------------------
@@ -122,6 +132,7 @@ struct Handle {
   double *fx = nullptr, *fy = nullptr, *fz = nullptr;
   double *rtmp[4] = {nullptr, nullptr, nullptr, nullptr};
   unsigned int *counts = nullptr;
+  BoxPair *box = nullptr;  // device: support of denx/psix/hpsix
   // spectra work buffers [H] complex
   double2 *spec[8] = {nullptr};
 
@@ -171,6 +182,11 @@ int field_poten(Handle *h);
 int field_forceimp(Handle *h);
 // potenimp + poten + forceimp; marks the fields valid
 int field_all(Handle *h);
+// impurity.cu: denx, psix, hpsix on the particle box; quantum force term;
+// reset of the box to the whole grid
+int impurity_density(Handle *h);
+int impurity_force_q(Handle *h);
+int impurity_reset_box(Handle *h);
 
 // dres: device array of 12 doubles: errHe, errimp, errvimp, then the 9 means
 int step_rk(Handle *h, double dt, double *dres);

@@ -19,6 +19,8 @@
 
 #include <algorithm>
 
+#include <cuda_pipeline.h>
+
 #include "common.cuh"
 #include "fft_reg.cuh"
 
@@ -486,13 +488,24 @@ __global__ void __launch_bounds__(kThreads) k_yz_reg(YRegArgs a) {
 }
 
 // z pass: one input per group, FFT_z once, then for each output
-// IFFT_z(coef * K(k) [* i D(k)] * X)
-template <int N>
+// IFFT_z(coef * K(k) [* i D(k)] * X).  The kernel values K of an output are
+// copied to shared memory with cp.async one output ahead (the first ones
+// before the input is even loaded), so their latency hides behind the FFT
+// work.  SINGLE: one output, multiplied in place (fewer registers).
+template <int N, bool SINGLE>
+static size_t smem_zconv() {
+  constexpr int N1 = RegShape<N>::N1, W = kThreads / N1;
+  return sizeof(double2) * ((size_t)N * W + N) + sizeof(double) * (SINGLE ? 1 : 2) * (size_t)N * W +
+         (sizeof(long) + 2 * sizeof(int)) * W;
+}
+
+template <int N, bool SINGLE>
 __global__ void __launch_bounds__(kThreads) k_zconv_reg(ZRegArgs a) {
   constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kThreads / N1;
   extern __shared__ double2 smem[];
   double2 *S = smem, *tw = smem + N * W;
-  long *offs = reinterpret_cast<long *>(tw + N);
+  double *Ks = reinterpret_cast<double *>(tw + N);  // [SINGLE ? 1 : 2][N][W]
+  long *offs = reinterpret_cast<long *>(Ks + (SINGLE ? 1 : 2) * N * W);
   int *kxs = reinterpret_cast<int *>(offs + W);
   int *kys = kxs + W;
   load_tw_n<N>(tw, a.tw);
@@ -503,9 +516,22 @@ __global__ void __launch_bounds__(kThreads) k_zconv_reg(ZRegArgs a) {
     kys[threadIdx.x] = o;
   }
   __syncthreads();
+  const ZGroup &G = a.g[blockIdx.x];
+  const int nout = SINGLE ? 1 : G.nout;
+  auto prefetch = [&](int o) {
+    const double *kern = G.o[o].kern;
+    if (!kern) return;
+    double *dst = Ks + (SINGLE ? 0 : (o & 1)) * N * W;
+    for (int e = threadIdx.x; e < N * W; e += kThreads) {
+      const int ww = e % W, k = e / W;
+      const long of = offs[ww];
+      if (of >= 0) __pipeline_memcpy_async(dst + e, kern + of + (long)k * a.sf, sizeof(double));
+    }
+  };
+  prefetch(0);
+  __pipeline_commit();
   const int w = threadIdx.x % W, j1 = threadIdx.x / W;
   const long off = offs[w];
-  const ZGroup &G = a.g[blockIdx.x];
   double2 v[N2];
 #pragma unroll
   for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? G.in[off + (j1 + N1 * j2) * a.sf] : make_double2(0.0, 0.0);
@@ -513,27 +539,33 @@ __global__ void __launch_bounds__(kThreads) k_zconv_reg(ZRegArgs a) {
   regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
   const double dx = (off >= 0) ? a.dsym[kxs[w]] : 0.0;
   const double dy = (off >= 0) ? a.dsym[a.nx + kys[w]] : 0.0;
-  for (int o = 0; o < G.nout; o++) {
+  for (int o = 0; o < nout; o++) {
+    if (!SINGLE && o + 1 < nout) prefetch(o + 1);
+    __pipeline_commit();
+    __pipeline_wait_prior(1);
+    __syncthreads();
     const ZOut Z = G.o[o];
-    double2 u[N2];
+    const double *K = Ks + (SINGLE ? 0 : (o & 1)) * N * W;
+    double2 u[SINGLE ? 1 : N2];
+    double2 *x = SINGLE ? v : u;
 #pragma unroll
     for (int c = 0; c < N2 / N1; c++)
 #pragma unroll
       for (int k1 = 0; k1 < N1; k1++) {
         const int k = (j1 + N1 * c) + N2 * k1;
         double cf = Z.coef;
-        if (Z.kern && off >= 0) cf *= __ldg(Z.kern + off + k * a.sf);
-        double2 x = cscale(v[c * N1 + k1], cf);
+        if (Z.kern && off >= 0) cf *= K[k * W + w];
+        double2 y = cscale(v[c * N1 + k1], cf);
         if (Z.dsym_axis >= 0) {
           const double ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
-          x = make_double2(-x.y * ds, x.x * ds);
+          y = make_double2(-y.y * ds, y.x * ds);
         }
-        u[c * N1 + k1] = x;
+        x[c * N1 + k1] = y;
       }
-    regfft::bwd2<N, N1, true>(u, S, lay, j1, tw);
+    regfft::bwd2<N, N1, true>(*reinterpret_cast<double2(*)[N2]>(x), S, lay, j1, tw);
     if (off >= 0) {
 #pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) Z.out[off + (j1 + N1 * n2) * a.sf] = u[n2];
+      for (int n2 = 0; n2 < N2; n2++) Z.out[off + (j1 + N1 * n2) * a.sf] = x[n2];
     }
   }
 }
@@ -618,7 +650,10 @@ template <int N>
 static int reg_attrs() {
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zconv<N, true>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zconv<N, false>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N>()));
   return HE4_OK;
@@ -829,11 +864,16 @@ int fft_z_conv(Handle *h, int n, const ZOp *ops) {
       a.tw = P.az.tw;
       for (int i = 0; i < nb; i++) a.g[i] = groups[g0 + i];
       const long total = (long)P.nxh * P.ny;
+      bool single = true;
+      for (int i = 0; i < nb; i++) single = single && (a.g[i].nout == 1);
       HE4_REG_SWITCH(P.nz, {
         constexpr int W = kThreads / RegShape<NN>::N1;
         a.map.W = W;
         dim3 grid(nb, (unsigned)((total + W - 1) / W));
-        k_zconv_reg<NN><<<grid, kThreads, smem_yz_reg<NN>(), h->stream>>>(a);
+        if (single)
+          k_zconv_reg<NN, true><<<grid, kThreads, smem_zconv<NN, true>(), h->stream>>>(a);
+        else
+          k_zconv_reg<NN, false><<<grid, kThreads, smem_zconv<NN, false>(), h->stream>>>(a);
       });
       HE4_LAUNCHED(h);
     }

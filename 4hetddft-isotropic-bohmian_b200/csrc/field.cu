@@ -13,73 +13,6 @@ namespace he4 {
 
 static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz}; }
 
-// ---------------------------------------------------------------------------
-// impurity density (denpart, potenimp.f90:294-338)
-// ---------------------------------------------------------------------------
-struct DepArgs {
-  int nx, ny, nz, npar;
-  double xmin, ymin, zmin, hx, hy, hz;
-};
-
-// NGP cell index as the reference computes it: int(1.5 + (r - r0)/h), 1-based
-__device__ __forceinline__ bool ngp_cell(const DepArgs &a, double rx, double ry, double rz, size_t *cell) {
-  const double fx = 1.5 + (rx - a.xmin) / a.hx;
-  const double fy = 1.5 + (ry - a.ymin) / a.hy;
-  const double fz = 1.5 + (rz - a.zmin) / a.hz;
-  if (!(fx > -1e9 && fx < 1e9 && fy > -1e9 && fy < 1e9 && fz > -1e9 && fz < 1e9)) return false;
-  const int ix = (int)fx, iy = (int)fy, iz = (int)fz;  // truncation toward zero
-  if (iz >= 1 && iz <= a.nz && iy >= 1 && iy <= a.ny && ix >= 1 && ix <= a.nx) {
-    *cell = ((size_t)(iz - 1) * a.ny + (iy - 1)) * a.nx + (ix - 1);
-    return true;
-  }
-  return false;
-}
-
-__global__ void k_deposit(const double *__restrict__ rimp, unsigned int *counts, DepArgs a) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= a.npar) return;
-  size_t cell;
-  if (ngp_cell(a, rimp[p], rimp[a.npar + p], rimp[2 * a.npar + p], &cell)) atomicAdd(counts + cell, 1u);
-}
-
-// denx = count / N_par / hxyz (potenimp.f90:322)
-__global__ void k_denx(const unsigned int *__restrict__ counts, double *denx, size_t n, double npar, double hxyz) {
-  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) denx[t] = (double)counts[t] / npar / hxyz;
-}
-
-// ironing (ironing.f90:19-28): interior points get 1/12 * (6 neighbours) +
-// 1/2 * centre, boundary points are copied.  Optionally writes sqrt.
-__global__ void k_iron(const double *__restrict__ src, double *dst, double *sqrt_out, Geo g) {
-  HE4_IJK(g);
-  double v;
-  if (i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1) {
-    const size_t sy = g.nx, sz = (size_t)g.nx * g.ny;
-    const double s6 = ((((src[t - 1] + src[t + 1]) + src[t - sy]) + src[t + sy]) + src[t - sz]) + src[t + sz];
-    // separately rounded products (no FMA) so denx is bit-identical to the
-    // reference's arithmetic
-    v = __dadd_rn(__dmul_rn(1.0 / 12.0, s6), __dmul_rn(0.5, src[t]));
-  } else {
-    v = src[t];
-  }
-  dst[t] = v;
-  if (sqrt_out) sqrt_out[t] = sqrt(v);
-}
-
-__global__ void k_sqrt(const double *__restrict__ src, double *dst, size_t n) {
-  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) dst[t] = sqrt(src[t]);
-}
-
-// out = scale * (d2x f + d2y f + d2z f)
-__global__ void k_lap_r(const double *__restrict__ f, double *out, double scale, Stencil st, Geo g) {
-  HE4_IJK(g);
-  const double a = stencil_axis(f, st.w2[0], st.m, g, i, j, k, 0);
-  const double b = stencil_axis(f, st.w2[1], st.m, g, i, j, k, 1);
-  const double c = stencil_axis(f, st.w2[2], st.m, g, i, j, k, 2);
-  out[t] = scale * ((a + b) + c);
-}
-
 // derden (derden.f90:26-28)
 __global__ void k_grad(const double *__restrict__ f, double *dx, double *dy, double *dz, Stencil st, Geo g) {
   HE4_IJK(g);
@@ -164,26 +97,8 @@ __global__ void k_pot4_final(double *pot4, const double *__restrict__ uimp, cons
 }
 
 // ---------------------------------------------------------------------------
-// forceimp pieces
+// gather of the force field at the particles
 // ---------------------------------------------------------------------------
-// f_i = (f_i + (1/denx)(d_i psix * hpsix - psix * d_i hpsix)) / m_X where
-// denx > 0 (potenimp.f90:52-69)
-__global__ void k_force_q(double *fx, double *fy, double *fz, const double *__restrict__ psix,
-                          const double *__restrict__ hpsix, const double *__restrict__ denx, double minv_unused,
-                          double mass, Stencil st, Geo g) {
-  HE4_IJK(g);
-  const double dn = denx[t];
-  const double inv = (dn > 0.0) ? 1.0 / dn : 0.0;
-  const double ps = psix[t], hp = hpsix[t];
-  double *F[3] = {fx, fy, fz};
-#pragma unroll
-  for (int ax = 0; ax < 3; ax++) {
-    const double dps = stencil_axis(psix, st.w1[ax], st.m, g, i, j, k, ax);
-    const double dhp = stencil_axis(hpsix, st.w1[ax], st.m, g, i, j, k, ax);
-    F[ax][t] = (F[ax][t] + inv * (dps * hp - ps * dhp)) / mass;
-  }
-}
-
 struct GatherArgs {
   int nx, ny, nz, npar;
   double x0, y0, z0, hx, hy, hz;
@@ -239,43 +154,8 @@ static OtArgs ot_args(const Handle *h) {
 static inline unsigned nblk(size_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
 int field_potenimp(Handle *h) {
-  const Geo g = geo(h);
-  const size_t N = h->N;
-  DepArgs d;
-  d.nx = h->nx;
-  d.ny = h->ny;
-  d.nz = h->nz;
-  d.npar = h->npar;
-  d.xmin = -h->p.xmax;
-  d.ymin = -h->p.ymax;
-  d.zmin = -h->p.zmax;
-  d.hx = h->hx;
-  d.hy = h->hy;
-  d.hz = h->hz;
-  HE4_CUDA_TRY(cudaMemsetAsync(h->counts, 0, sizeof(unsigned int) * N, h->stream));
-  k_deposit<<<nblk(h->npar), 256, 0, h->stream>>>(h->rimp, h->counts, d);
-  HE4_LAUNCHED(h);
-  const double hxyz = h->hx * h->hy * h->hz;
-  k_denx<<<nblk(N), 256, 0, h->stream>>>(h->counts, h->denx, N, (double)h->npar, hxyz);
-  HE4_LAUNCHED(h);
-  if (h->p.ironx <= 0) {
-    k_sqrt<<<nblk(N), 256, 0, h->stream>>>(h->denx, h->psix, N);
-    HE4_LAUNCHED(h);
-  } else {
-    for (int it = 0; it < h->p.ironx; it++) {
-      // ping-pong through rtmp[0]; the last pass lands in denx and writes psix
-      double *src = (it % 2 == 0) ? h->denx : h->rtmp[0];
-      double *dst = (it % 2 == 0) ? h->rtmp[0] : h->denx;
-      const bool last = (it == h->p.ironx - 1);
-      k_iron<<<grid3(g), block3(), 0, h->stream>>>(src, dst, last ? h->psix : nullptr, g);
-      HE4_LAUNCHED(h);
-      if (last && dst != h->denx) {
-        HE4_CUDA_TRY(cudaMemcpyAsync(h->denx, dst, sizeof(double) * N, cudaMemcpyDeviceToDevice, h->stream));
-      }
-    }
-  }
-  k_lap_r<<<grid3(g), block3(), 0, h->stream>>>(h->psix, h->hpsix, -h->h2o2mx, h->st, g);
-  HE4_LAUNCHED(h);
+  // denpart: denx, psix, hpsix on the particle box (impurity.cu)
+  HE4_TRY(impurity_density(h));
   // uimp = IFFT(FFT(denx) * Vq) * renor (potenimp.f90:17-19)
   const double *in[1] = {h->denx};
   double2 *sp[1] = {h->spec[1]};
@@ -366,18 +246,19 @@ int field_poten(Handle *h) {
 
 int field_forceimp(Handle *h) {
   const Geo g = geo(h);
-  // f_i = -IFFT(FFT(d_i rho) Vq) * renor = IFFT(-renor Vq i D_i fden)
-  // (potenimp.f90:42-50)
-  ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, -h->renor, 0},
-                {h->spec[0], h->spec[2], h->vq, -h->renor, 1},
-                {h->spec[0], h->spec[3], h->vq, -h->renor, 2}};
+  // f_i = -IFFT(FFT(d_i rho) Vq) * renor / m_X = IFFT(-renor/m_X Vq i D_i fden)
+  // (potenimp.f90:42-50, with the 1/m_X of :67-69 folded in)
+  (void)g;
+  const double c = -h->renor / h->mAg_u;
+  ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, c, 0},
+                {h->spec[0], h->spec[2], h->vq, c, 1},
+                {h->spec[0], h->spec[3], h->vq, c, 2}};
   HE4_TRY(fft_z_conv(h, 3, ops));
   double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
   double *out[3] = {h->fx, h->fy, h->fz};
   HE4_TRY(fft_c2r(h, 3, sp, out));
-  k_force_q<<<grid3(g), block3(), 0, h->stream>>>(h->fx, h->fy, h->fz, h->psix, h->hpsix, h->denx, 0.0, h->mAg_u,
-                                                  h->st, g);
-  HE4_LAUNCHED(h);
+  // quantum-potential term, nonzero only where denx > 0 (impurity.cu)
+  HE4_TRY(impurity_force_q(h));
   GatherArgs a;
   a.nx = h->nx;
   a.ny = h->ny;
