@@ -86,6 +86,7 @@ static int dalloc(T **p, size_t n) {
 }
 
 static void free_all(Handle *h) {
+  free_graphs(h);
   fft_plan_free(h->fft);
   void *ptrs[] = {h->wcgk, h->fvlj4, h->kalfs, h->vq, h->pmod, h->dsym, h->timec_re, h->psi, h->psiold[0],
                   h->psiold[1], h->psiold[2], h->hpsiold[0], h->hpsiold[1], h->pc, h->q, h->ctmp, h->den, h->pot4,
@@ -333,7 +334,7 @@ int he4_poten(he4_handle *hh) {
 int he4_forceimp(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
-  HE4_TRY(field_forceimp(h));
+  HE4_TRY(field_forceimp(h, true));
   h->field_valid = 1;  // potenimp, poten, forceimp: the reference's sequence
   return sync_and_check(h);
 }
@@ -399,11 +400,14 @@ int he4_run(he4_handle *hh, int32_t nsteps, double deltat, double *err, double *
   double *dres = nullptr;
   HE4_CUDA_TRY(cudaMallocAsync((void **)&dres, sizeof(double) * 12 * nsteps, h->stream));
   int e = HE4_OK;
-  for (int s = 0; s < nsteps && e == HE4_OK; s++) {
-    if (h->nsteps_done < 3)
-      e = step_rk(h, deltat, dres + 12 * s);
-    else
-      e = step_pc(h, deltat, dres + 12 * s);
+  int s = 0;
+  for (; s < nsteps && e == HE4_OK && h->nsteps_done < 3; s++) e = step_rk(h, deltat, dres + 12 * s);
+  if (e == HE4_OK && s < nsteps) {
+    if (h->use_graphs) {
+      e = run_pc_graphs(h, nsteps - s, deltat, dres + 12 * s);
+    } else {
+      for (; s < nsteps && e == HE4_OK; s++) e = step_pc(h, deltat, dres + 12 * s);
+    }
   }
   double *hres = nullptr;
   if (e == HE4_OK) {
@@ -482,9 +486,14 @@ int he4_get_field(he4_handle *hh, int32_t which, double *out) {
     case HE4_F_DXDEN: src = h->dxden; break;
     case HE4_F_DYDEN: src = h->dyden; break;
     case HE4_F_DZDEN: src = h->dzden; break;
-    case HE4_F_FX: src = h->fx; break;
-    case HE4_F_FY: src = h->fy; break;
-    case HE4_F_FZ: src = h->fz; break;
+    case HE4_F_FX:
+    case HE4_F_FY:
+    case HE4_F_FZ:
+      // a time step computes the force field only where the particles read
+      // it; complete it from the density spectrum of the same evaluation
+      if (h->field_valid && !h->forces_full) HE4_TRY(field_forces(h, true));
+      src = (which == HE4_F_FX) ? h->fx : (which == HE4_F_FY) ? h->fy : h->fz;
+      break;
     case HE4_F_PENALTY: src = h->penalty; break;
     case HE4_F_CORR: src = h->corr; break;
     default:

@@ -5,6 +5,7 @@
 #include <stdio.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/he4_tddft.h"
 
@@ -104,6 +105,25 @@ struct BoxPair {
 };
 
 // ---------------------------------------------------------------------------
+// host-side step state: which buffer holds which history level, the ring
+// indices of steppc and the time step.  A captured PC step is valid for the
+// state it started from and leaves the state it was captured to.
+// ---------------------------------------------------------------------------
+struct StepState {
+  double2 *psi, *psiold[3], *hpsiold[2], *ctmp;
+  double *rimpold[3], *vimpold[3], *aimpold[2];
+  int ioldp[3], ioldh[2], ioldr[3], ioldv[3], iolda[2];
+  double dt;
+};
+
+struct StepGraph {
+  StepState before, after;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t kernels = 0;
+};
+
+// ---------------------------------------------------------------------------
 // the handle
 // ---------------------------------------------------------------------------
 struct Handle {
@@ -152,7 +172,12 @@ struct Handle {
   // pot4, aimp and the other fields belong to the current psi and rimp
   // (the field evaluation that DFT4He3d.f90:630-634 does before the loop)
   int field_valid = 0;
+  // fx, fy, fz hold the whole grid (otherwise only the force box)
+  int forces_full = 0;
   size_t red_len = 0;
+  // captured PC steps (one per distinct StepState; the states repeat)
+  std::vector<StepGraph> graphs;
+  int use_graphs = 1;
 };
 
 // kernel-level entry points used by the ABI layer
@@ -168,8 +193,28 @@ struct ZOp {
   double coef;
   int dsym_axis;  // -1 none, 0/1/2: multiply by i*dsym[axis](k)
   int mode = 0;   // 0: FFT_z, multiply, IFFT_z; 1: FFT_z only; 2: IFFT_z only
+  int boxz = 0;   // store only the z planes of the force box (see force_range)
 };
 int fft_z_conv(Handle *h, int n, const ZOp *ops);
+// inverse y and x passes restricted to the pencils and rows of the force box
+int fft_c2r_box(Handle *h, int n, double2 *const *in, double *const *out);
+
+// The cells where the force field is needed: the impurity box widened by one
+// cell (the trilinear gather reads cells floor(a) and floor(a)+1 around the
+// NGP cell).  Whole axis when the box is full; lo > hi when it is empty.
+__device__ __forceinline__ void force_range(const BoxPair *bp, int axis, int n, int *lo, int *hi) {
+  const Box b = bp->cur;
+  if (b.full) {
+    *lo = 0;
+    *hi = n - 1;
+  } else if (b.empty) {
+    *lo = 1;
+    *hi = 0;
+  } else {
+    *lo = max(0, b.lo[axis] - 1);
+    *hi = min(n - 1, b.hi[axis] + 1);
+  }
+}
 // plain transform along z of one half spectrum, in place
 int fft_z_only(Handle *h, double2 *buf, bool inverse);
 // x pass alone (R2C: rin -> cout; C2R: cin -> rout)
@@ -179,7 +224,10 @@ int setup_kernels(Handle *h);
 
 int field_potenimp(Handle *h);
 int field_poten(Handle *h);
-int field_forceimp(Handle *h);
+// full: the force field on the whole grid; otherwise only where the gather
+// reads it (a time step's need).  field_forces recomputes just the field.
+int field_forceimp(Handle *h, bool full);
+int field_forces(Handle *h, bool full);
 // potenimp + poten + forceimp; marks the fields valid
 int field_all(Handle *h);
 // impurity.cu: denx, psix, hpsix on the particle box; quantum force term;
@@ -191,6 +239,10 @@ int impurity_reset_box(Handle *h);
 // dres: device array of 12 doubles: errHe, errimp, errvimp, then the 9 means
 int step_rk(Handle *h, double dt, double *dres);
 int step_pc(Handle *h, double dt, double *dres);
+// n PC steps from captured graphs (capturing the states not seen yet);
+// results of step s land in dres[12 s .. 12 s + 11]
+int run_pc_graphs(Handle *h, int n, double dt, double *dres);
+void free_graphs(Handle *h);
 int compute_energy(Handle *h, he4_energies *e);
 int compute_diagnostics(Handle *h, int n4, double *host_out);
 int compute_den(Handle *h);

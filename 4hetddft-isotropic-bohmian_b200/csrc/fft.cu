@@ -409,6 +409,7 @@ struct ZOut {
   const double *kern;
   double coef;
   int dsym_axis;
+  int boxz;  // store only the z planes of the force box
 };
 struct ZGroup {
   const double2 *in;
@@ -420,15 +421,18 @@ struct YRegArgs {
   PencilMap map;
   long sf;
   const double2 *tw;
+  const BoxPair *box;  // non-null: only pencils whose z lies in the force box
+  int nz;
   double2 *buf[kMaxBatch];
 };
 
 struct ZRegArgs {
   PencilMap map;
   long sf;
-  int nx, ny;
+  int nx, ny, nz;
   const double *dsym;
   const double2 *tw;
+  const BoxPair *box;  // for outputs with boxz
   ZGroup g[kMaxBatch];
 };
 
@@ -437,6 +441,8 @@ struct XRegArgs {
   long nrow;
   double scale;
   const double2 *tw;
+  const BoxPair *box;  // non-null (C2R): only rows (y, z) inside the force box
+  int ny, nz;
   const double *rin[kMaxBatch];
   double2 *cout[kMaxBatch];
   const double2 *cin[kMaxBatch];
@@ -467,11 +473,22 @@ __global__ void __launch_bounds__(kThreads) k_yz_reg(YRegArgs a) {
   double2 *S = smem, *tw = smem + N * W;
   long *offs = reinterpret_cast<long *>(tw + N);
   load_tw_n<N>(tw, a.tw);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
   if (threadIdx.x < W) {
     int kx, o;
-    offs[threadIdx.x] = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
+    long of = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
+    if (a.box && of >= 0) {  // pencils along y at plane z = o
+      int lo, hi;
+      force_range(a.box, 2, a.nz, &lo, &hi);
+      if (o < lo || o > hi) of = -1;
+    }
+    offs[threadIdx.x] = of;
+    if (of >= 0) any = 1;
   }
   __syncthreads();
+  if (!any) return;
   const int w = threadIdx.x % W, j1 = threadIdx.x / W;
   const long off = offs[w];
   double2 *data = a.buf[blockIdx.y];
@@ -564,8 +581,13 @@ __global__ void __launch_bounds__(kThreads) k_zconv_reg(ZRegArgs a) {
       }
     regfft::bwd2<N, N1, true>(*reinterpret_cast<double2(*)[N2]>(x), S, lay, j1, tw);
     if (off >= 0) {
+      int zlo = 0, zhi = N - 1;
+      if (Z.boxz) force_range(a.box, 2, a.nz, &zlo, &zhi);
 #pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) Z.out[off + (j1 + N1 * n2) * a.sf] = x[n2];
+      for (int n2 = 0; n2 < N2; n2++) {
+        const int z = j1 + N1 * n2;
+        if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+      }
     }
   }
 }
@@ -615,12 +637,23 @@ __global__ void __launch_bounds__(kThreads) k_xc2r_reg(XRegArgs a) {
   load_tw_n<N>(tw, a.tw);
   const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
   const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
+  // rows outside the force box (when restricted) are neither read nor written
+  bool ina = ra < a.nrow, inb = rb < a.nrow;
+  if (a.box) {
+    int ylo, yhi, zlo, zhi;
+    force_range(a.box, 1, a.ny, &ylo, &yhi);
+    force_range(a.box, 2, a.nz, &zlo, &zhi);
+    const int ya = (int)(ra % a.ny), za = (int)(ra / a.ny), yb = (int)(rb % a.ny), zb = (int)(rb / a.ny);
+    ina = ina && ya >= ylo && ya <= yhi && za >= zlo && za <= zhi;
+    inb = inb && yb >= ylo && yb <= yhi && zb >= zlo && zb <= zhi;
+    if (!__syncthreads_or(ina || inb)) return;
+  }
   const double2 *in = a.cin[blockIdx.y];
   double *out = a.rout[blockIdx.y];
   double2 *Sp = S + p * SP;
   for (int k = j1; k < a.nxh; k += N1) {
-    double2 X = (ra < a.nrow) ? in[ra * a.nxh + k] : make_double2(0.0, 0.0);
-    double2 Y = (rb < a.nrow) ? in[rb * a.nxh + k] : make_double2(0.0, 0.0);
+    double2 X = ina ? in[ra * a.nxh + k] : make_double2(0.0, 0.0);
+    double2 Y = inb ? in[rb * a.nxh + k] : make_double2(0.0, 0.0);
     if (k == 0 || 2 * k == N) {  // DC / Nyquist of a real transform: drop Im
       X.y = 0.0;
       Y.y = 0.0;
@@ -641,8 +674,8 @@ __global__ void __launch_bounds__(kThreads) k_xc2r_reg(XRegArgs a) {
 #pragma unroll
   for (int n2 = 0; n2 < N2; n2++) {
     const int x = j1 + N1 * n2;
-    if (ra < a.nrow) out[ra * N + x] = v[n2].x * sc;
-    if (rb < a.nrow) out[rb * N + x] = v[n2].y * sc;
+    if (ina) out[ra * N + x] = v[n2].x * sc;
+    if (inb) out[rb * N + x] = v[n2].y * sc;
   }
 }
 
@@ -712,8 +745,9 @@ void fft_plan_free(FftPlan &P) {
   P.ax.tw = P.ay.tw = P.az.tw = nullptr;
 }
 
+// box (C2R only, register path): restrict to the rows of the force box
 static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *cout, double2 *const *cin,
-                  double *const *rout, bool inverse) {
+                  double *const *rout, bool inverse, const BoxPair *box = nullptr) {
   const FftPlan &P = h->fft;
   const long nrow = (long)P.ny * P.nz;
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
@@ -724,6 +758,9 @@ static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *co
       a.nrow = nrow;
       a.scale = 1.0;
       a.tw = P.ax.tw;
+      a.box = inverse ? box : nullptr;
+      a.ny = P.ny;
+      a.nz = P.nz;
       for (int i = 0; i < nb; i++) {
         if (inverse) {
           a.cin[i] = cin[b0 + i];
@@ -768,8 +805,10 @@ static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *co
   return HE4_OK;
 }
 
-// in-place complex transform of every pencil along y (axis 1) or z (axis 2)
-static int strided_pass(Handle *h, int n, double2 *const *buf, int axis, bool inverse) {
+// in-place complex transform of every pencil along y (axis 1) or z (axis 2);
+// box (y pass, register path): only pencils whose z lies in the force box
+static int strided_pass(Handle *h, int n, double2 *const *buf, int axis, bool inverse,
+                        const BoxPair *box = nullptr) {
   const FftPlan &P = h->fft;
   const int len = (axis == 1) ? P.ny : P.nz;
   const AxisPlan &A = (axis == 1) ? P.ay : P.az;
@@ -785,6 +824,8 @@ static int strided_pass(Handle *h, int n, double2 *const *buf, int axis, bool in
       YRegArgs a{};
       a.sf = sf;
       a.tw = A.tw;
+      a.box = (axis == 1) ? box : nullptr;
+      a.nz = P.nz;
       for (int i = 0; i < nb; i++) a.buf[i] = buf[b0 + i];
       HE4_REG_SWITCH(len, {
         constexpr int W = kThreads / RegShape<NN>::N1;
@@ -834,6 +875,12 @@ int fft_c2r(Handle *h, int n, double2 *const *in, double *const *out) {
   return HE4_OK;
 }
 
+int fft_c2r_box(Handle *h, int n, double2 *const *in, double *const *out) {
+  HE4_TRY(strided_pass(h, n, in, 1, true, h->box));
+  HE4_TRY(x_pass(h, n, nullptr, nullptr, in, out, true, h->box));
+  return HE4_OK;
+}
+
 int fft_z_conv(Handle *h, int n, const ZOp *ops) {
   const FftPlan &P = h->fft;
   if (n <= 0) return HE4_OK;
@@ -849,7 +896,7 @@ int fft_z_conv(Handle *h, int n, const ZOp *ops) {
         ng++;
       }
       ZGroup &g = groups[ng - 1];
-      g.o[g.nout++] = ZOut{ops[i].out, ops[i].kern, ops[i].coef, ops[i].dsym_axis};
+      g.o[g.nout++] = ZOut{ops[i].out, ops[i].kern, ops[i].coef, ops[i].dsym_axis, ops[i].boxz};
     }
     for (int g0 = 0; g0 < ng; g0 += kMaxBatch) {
       const int nb = std::min(kMaxBatch, ng - g0);
@@ -860,8 +907,10 @@ int fft_z_conv(Handle *h, int n, const ZOp *ops) {
       a.sf = (long)P.ny * P.nxh;
       a.nx = P.nx;
       a.ny = P.ny;
+      a.nz = P.nz;
       a.dsym = h->dsym;
       a.tw = P.az.tw;
+      a.box = h->box;
       for (int i = 0; i < nb; i++) a.g[i] = groups[g0 + i];
       const long total = (long)P.nxh * P.ny;
       bool single = true;

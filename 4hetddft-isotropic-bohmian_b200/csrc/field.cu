@@ -244,21 +244,32 @@ int field_poten(Handle *h) {
   return HE4_OK;
 }
 
-int field_forceimp(Handle *h) {
-  const Geo g = geo(h);
+// The force field f_i on the grid: the whole grid (full) or only the cells
+// the trilinear gather reads (the impurity box widened by one cell), which
+// is what a time step needs.
+int field_forces(Handle *h, bool full) {
   // f_i = -IFFT(FFT(d_i rho) Vq) * renor / m_X = IFFT(-renor/m_X Vq i D_i fden)
   // (potenimp.f90:42-50, with the 1/m_X of :67-69 folded in)
-  (void)g;
   const double c = -h->renor / h->mAg_u;
-  ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, c, 0},
-                {h->spec[0], h->spec[2], h->vq, c, 1},
-                {h->spec[0], h->spec[3], h->vq, c, 2}};
+  const int bz = full ? 0 : 1;
+  ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, c, 0, 0, bz},
+                {h->spec[0], h->spec[2], h->vq, c, 1, 0, bz},
+                {h->spec[0], h->spec[3], h->vq, c, 2, 0, bz}};
   HE4_TRY(fft_z_conv(h, 3, ops));
   double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
   double *out[3] = {h->fx, h->fy, h->fz};
-  HE4_TRY(fft_c2r(h, 3, sp, out));
+  if (full)
+    HE4_TRY(fft_c2r(h, 3, sp, out));
+  else
+    HE4_TRY(fft_c2r_box(h, 3, sp, out));
   // quantum-potential term, nonzero only where denx > 0 (impurity.cu)
   HE4_TRY(impurity_force_q(h));
+  h->forces_full = full ? 1 : 0;
+  return HE4_OK;
+}
+
+int field_forceimp(Handle *h, bool full) {
+  HE4_TRY(field_forces(h, full));
   GatherArgs a;
   a.nx = h->nx;
   a.ny = h->ny;

@@ -11,6 +11,8 @@
 //  * corrector: psi_{n+1} goes to a scratch buffer that is swapped with psi.
 // Each kernel evaluates the complex Laplacian of its input (npd-point
 // periodic stencils) and H psi = timec*(h2o2m4*lap - pot4*psi) in registers.
+#include <string.h>
+
 #include <utility>
 
 #include "common.cuh"
@@ -255,7 +257,7 @@ int field_all(Handle *h) {
   h->field_valid = 0;
   HE4_TRY(field_potenimp(h));
   HE4_TRY(field_poten(h));
-  HE4_TRY(field_forceimp(h));
+  HE4_TRY(field_forceimp(h, false));
   h->field_valid = 1;
   return HE4_OK;
 }
@@ -354,6 +356,127 @@ int step_pc(Handle *h, double dt, double *dres) {
   HE4_TRY(field_all(h));
   HE4_TRY(particle_means(h, dres + 3));
   h->nsteps_done++;
+  return HE4_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graphs of the PC step
+// ---------------------------------------------------------------------------
+static StepState get_step_state(const Handle *h, double dt) {
+  StepState s;
+  memset(&s, 0, sizeof(s));
+  s.psi = h->psi;
+  s.ctmp = h->ctmp;
+  for (int i = 0; i < 3; i++) {
+    s.psiold[i] = h->psiold[i];
+    s.rimpold[i] = h->rimpold[i];
+    s.vimpold[i] = h->vimpold[i];
+    s.ioldp[i] = h->ioldp[i];
+    s.ioldr[i] = h->ioldr[i];
+    s.ioldv[i] = h->ioldv[i];
+  }
+  for (int i = 0; i < 2; i++) {
+    s.hpsiold[i] = h->hpsiold[i];
+    s.aimpold[i] = h->aimpold[i];
+    s.ioldh[i] = h->ioldh[i];
+    s.iolda[i] = h->iolda[i];
+  }
+  s.dt = dt;
+  return s;
+}
+
+static void set_step_state(Handle *h, const StepState &s) {
+  h->psi = s.psi;
+  h->ctmp = s.ctmp;
+  for (int i = 0; i < 3; i++) {
+    h->psiold[i] = s.psiold[i];
+    h->rimpold[i] = s.rimpold[i];
+    h->vimpold[i] = s.vimpold[i];
+    h->ioldp[i] = s.ioldp[i];
+    h->ioldr[i] = s.ioldr[i];
+    h->ioldv[i] = s.ioldv[i];
+  }
+  for (int i = 0; i < 2; i++) {
+    h->hpsiold[i] = s.hpsiold[i];
+    h->aimpold[i] = s.aimpold[i];
+    h->ioldh[i] = s.ioldh[i];
+    h->iolda[i] = s.iolda[i];
+  }
+}
+
+void free_graphs(Handle *h) {
+  for (StepGraph &g : h->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  h->graphs.clear();
+}
+
+constexpr size_t kMaxGraphs = 24;
+
+// Capture one PC step from the current state (results into h->scal).  The
+// host state advances exactly as an eager step would; the graph has not run.
+static int capture_pc(Handle *h, double dt, StepGraph *out) {
+  StepGraph g;
+  g.before = get_step_state(h, dt);
+  const int64_t l0 = h->launches;
+  const int done0 = h->nsteps_done;
+  HE4_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = step_pc(h, dt, h->scal);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+  h->nsteps_done = done0;
+  g.kernels = h->launches - l0;
+  h->launches = l0;
+  if (rc != HE4_OK || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    set_step_state(h, g.before);
+    if (rc == HE4_OK) set_error("stream capture of the PC step: %s", cudaGetErrorString(ce));
+    cudaGetLastError();
+    return rc != HE4_OK ? rc : HE4_E_CUDA;
+  }
+  g.graph = graph;
+  const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (ie != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    set_step_state(h, g.before);
+    set_error("graph instantiation: %s", cudaGetErrorString(ie));
+    return HE4_E_CUDA;
+  }
+  g.after = get_step_state(h, dt);
+  *out = g;
+  return HE4_OK;
+}
+
+int run_pc_graphs(Handle *h, int n, double dt, double *dres) {
+  if (!h->field_valid) HE4_TRY(field_all(h));
+  for (int s = 0; s < n; s++) {
+    const StepState now = get_step_state(h, dt);
+    StepGraph *hit = nullptr;
+    for (StepGraph &g : h->graphs)
+      if (memcmp(&g.before, &now, sizeof(StepState)) == 0) {
+        hit = &g;
+        break;
+      }
+    if (!hit && h->graphs.size() < kMaxGraphs) {
+      StepGraph g;
+      HE4_TRY(capture_pc(h, dt, &g));
+      set_step_state(h, g.before);
+      h->graphs.push_back(g);
+      hit = &h->graphs.back();
+    }
+    if (hit) {
+      HE4_CUDA_TRY(cudaGraphLaunch(hit->exec, h->stream));
+      h->launches += hit->kernels;
+      set_step_state(h, hit->after);
+      h->nsteps_done++;
+      h->field_valid = 1;
+      HE4_CUDA_TRY(cudaMemcpyAsync(dres + 12 * (size_t)s, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   h->stream));
+    } else {
+      HE4_TRY(step_pc(h, dt, dres + 12 * (size_t)s));
+    }
+  }
   return HE4_OK;
 }
 

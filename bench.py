@@ -263,9 +263,17 @@ def kernel_roofline(pkg, g, stream, args):
         return None
     peak, src = load_peaks()
     achieved = byts.value / (ms.value * 1e-3) / 1e9
-    return {"kernel": name.value.decode(), "bound": "hbm", "achieved": achieved, "peak": peak,
+    kname = name.value.decode()
+    # DRAM bytes per launch of this kernel from the committed ncu capture of
+    # the same launch at 256^3 (profiles/fft_passes_c3.md)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "fft_passes_c3.json")
+    if args.config == "c3" and os.path.exists(prof):
+        traffic = json.load(open(prof))["traffic_bytes_per_launch"].get(kname)
+    return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src,
-            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "traffic_source": "ncu dram__bytes, profiles/fft_passes_c3.md" if traffic else None,
             "bytes_per_launch": byts.value, "ms_per_launch": ms.value}
 
 

@@ -146,17 +146,24 @@ def test_run_equals_single_steps_and_is_deterministic(pkg, c1):
         assert np.array_equal(np.array(es), e1[3:])
 
 
-@pytest.mark.parametrize("variant", ["npd13", "ot_core", "noncubic"])
+@pytest.mark.parametrize("variant", ["npd13", "ot_core", "noncubic", "edge"])
 def test_field_parity_variants(pkg, ora, variant):
+    """Other stencil widths, the 'OT ' core, a non-cubic grid, and particles
+    next to a face of the grid (the impurity box falls back to the whole
+    grid there)."""
     w = pkg.workloads
+    center = (0.0, 0.0, 2.0)
     if variant == "npd13":
         p = w.make_params(48, 0.6, 64, npd=13)
     elif variant == "ot_core":
         p = w.make_params(48, 0.6, 64, core4=pkg.abi.HE4_CORE_OT)
+    elif variant == "edge":
+        p = w.make_params(48, 0.6, 64)
+        center = (0.0, 0.0, p.zmax - 1.5)
     else:
         p = w.make_params(40, 0.6, 64, ny=48, nz=60)
     psi = w.droplet_psi(p, 150)
-    r, v = w.particles(p.n_par, 5, 100.0)
+    r, v = w.particles(p.n_par, 5, 100.0, center=center)
     o = ora.Oracle(p)
     vq = o.get_kernel("vq")
     o.set_state(psi, r, v)
