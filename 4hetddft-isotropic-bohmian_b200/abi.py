@@ -22,6 +22,7 @@ HE4_POT_MORSE = 1
 HE4_POT_NULL = 2
 
 HE4_PREC_FP64 = 0
+HE4_PREC_FP32CONV = 1
 
 FIELDS = [
     "den", "pot4", "denx", "psix", "hpsix", "uimp", "dencg", "delj4", "denalf",

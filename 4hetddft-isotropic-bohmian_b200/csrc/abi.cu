@@ -67,9 +67,17 @@ static int check_params(const he4_params *p) {
     set_error("unknown pot_kind %d", p->pot_kind);
     return HE4_E_ARG;
   }
-  if (p->precision != HE4_PREC_FP64) {
+  if (p->precision != HE4_PREC_FP64 && p->precision != HE4_PREC_FP32CONV) {
     set_error("precision mode %d is not implemented", p->precision);
     return HE4_E_UNSUPPORTED;
+  }
+  if (p->precision == HE4_PREC_FP32CONV) {
+    auto reg = [](int n) { return n >= 16 && n <= 256 && (n & (n - 1)) == 0; };
+    if (!reg(p->nx) || !reg(p->ny) || !reg(p->nz)) {
+      set_error("the FP32-convolution form needs power-of-two axes in [16, 256] (got %d x %d x %d)", p->nx, p->ny,
+                p->nz);
+      return HE4_E_UNSUPPORTED;
+    }
   }
   return HE4_OK;
 }
@@ -94,7 +102,8 @@ static void free_all(Handle *h) {
                   h->dyden, h->dzden, h->penalty, h->corr, h->denx, h->psix, h->hpsix, h->uimp, h->fx, h->fy,
                   h->fz, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], h->counts, h->rimp, h->vimp, h->aimp,
                   h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
-                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->box};
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->box,
+                  h->k32[0], h->k32[1], h->k32[2], h->k32[3], h->dsym32};
   for (void *p : ptrs) cudaFree(p);
   for (int i = 0; i < 8; i++) cudaFree(h->spec[i]);
   if (h->hscal) cudaFreeHost(h->hscal);
@@ -147,6 +156,11 @@ static int create(const he4_params *pin, Handle *h) {
   HE4_TRY(dalloc(&h->pmod, H));
   HE4_TRY(dalloc(&h->dsym, (size_t)p.nx + p.ny + p.nz));
   HE4_TRY(dalloc(&h->timec_re, (size_t)p.nz));
+  h->fp32 = (p.precision == HE4_PREC_FP32CONV);
+  if (h->fp32) {
+    for (int i = 0; i < 4; i++) HE4_TRY(dalloc(&h->k32[i], H));
+    HE4_TRY(dalloc(&h->dsym32, (size_t)p.nx + p.ny + p.nz));
+  }
   double2 **cfields[] = {&h->psi, &h->psiold[0], &h->psiold[1], &h->psiold[2], &h->hpsiold[0],
                          &h->hpsiold[1], &h->pc, &h->q, &h->ctmp};
   for (double2 **f : cfields) HE4_TRY(dalloc(f, N));
@@ -535,9 +549,13 @@ int he4_fft_r2c(he4_handle *hh, const double *in, double *out) {
   }
   HE4_CUDA_TRY(cudaMemcpyAsync(h->rtmp[0], in, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
   const double *src[1] = {h->rtmp[0]};
-  double2 *dst[1] = {h->spec[4] ? h->spec[4] : h->spec[1]};
+  double2 *dst[1] = {h->spec[1]};
   HE4_TRY(fft_r2c(h, 1, src, dst));
   HE4_TRY(fft_z_only(h, dst[0], false));
+  if (h->fp32) {  // FP32 half spectrum -> FP64 for the caller
+    HE4_TRY(widen(h, reinterpret_cast<const float *>(h->spec[1]), reinterpret_cast<double *>(h->spec[2]), 2 * h->H));
+    dst[0] = h->spec[2];
+  }
   HE4_CUDA_TRY(cudaMemcpyAsync(out, dst[0], sizeof(double2) * h->H, cudaMemcpyDeviceToHost, h->stream));
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return HE4_OK;
@@ -549,8 +567,13 @@ int he4_fft_c2r(he4_handle *hh, const double *in, double *out) {
     set_error("null buffer");
     return HE4_E_ARG;
   }
-  double2 *buf = h->spec[4] ? h->spec[4] : h->spec[1];
-  HE4_CUDA_TRY(cudaMemcpyAsync(buf, in, sizeof(double2) * h->H, cudaMemcpyHostToDevice, h->stream));
+  double2 *buf = h->spec[1];
+  if (h->fp32) {  // the caller's FP64 half spectrum, rounded to FP32
+    HE4_CUDA_TRY(cudaMemcpyAsync(h->spec[2], in, sizeof(double2) * h->H, cudaMemcpyHostToDevice, h->stream));
+    HE4_TRY(narrow(h, reinterpret_cast<const double *>(h->spec[2]), reinterpret_cast<float *>(buf), 2 * h->H));
+  } else {
+    HE4_CUDA_TRY(cudaMemcpyAsync(buf, in, sizeof(double2) * h->H, cudaMemcpyHostToDevice, h->stream));
+  }
   HE4_TRY(fft_z_only(h, buf, true));
   double2 *src[1] = {buf};
   double *dst[1] = {h->rtmp[0]};
@@ -597,9 +620,11 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
   static const char *names[7] = {"k_fft_z_conv",  "k_fft_y",           "k_fft_x_r2c", "k_fft_x_c2r",
                                  "k_fft_z_plain", "k_fft_z_conv_nokern", "k_fft_z_conv_3out"};
   const double H = (double)h->H, N = (double)h->N;
-  // algorithmic bytes: read input once, write output once (+ the real kernel)
-  const double bytes[7] = {16 * H + 8 * H + 16 * H, 2 * 16 * H, 8 * N + 16 * H, 16 * H + 8 * N,
-                           2 * 16 * H, 2 * 16 * H, 16 * H + 3 * (8 * H + 16 * H)};
+  // algorithmic bytes: read input once, write output once (+ the real
+  // kernel); c and k are the sizes of a spectrum and a kernel element
+  const double c = h->fp32 ? 8 : 16, k = h->fp32 ? 4 : 8;
+  const double bytes[7] = {c * H + k * H + c * H, 2 * c * H, 8 * N + c * H, c * H + 8 * N,
+                           2 * c * H,             2 * c * H, c * H + 3 * (k * H + c * H)};
   if (which < 0 || which > 6) {
     set_error("unknown kernel id %d", which);
     return HE4_E_ARG;

@@ -69,7 +69,8 @@ struct AxisPlan {
   int n = 0;
   int nst = 0;
   int radix[kMaxStages] = {0};
-  double2 *tw = nullptr;  // device: exp(-2 pi i t / n), t in [0, n)
+  double2 *tw = nullptr;   // device: exp(-2 pi i t / n), t in [0, n)
+  float2 *tw32 = nullptr;  // the same, rounded to FP32 (FP32-convolution form)
 };
 
 struct FftPlan {
@@ -136,6 +137,21 @@ struct Handle {
   int64_t launches = 0;
   FftPlan fft;
   Stencil st;
+
+  // FP32-convolution form: spectra hold float2, the k-space multiply uses
+  // FP32 copies of the kernels and of the derivative symbol
+  int fp32 = 0;
+  float *k32[4] = {nullptr, nullptr, nullptr, nullptr};  // wcgk, fvlj4, kalfs, vq
+  float *dsym32 = nullptr;
+  // FP32 twin of one of the FP64 kernel arrays (nullptr for nullptr)
+  const float *kern32(const double *k) const {
+    if (!k) return nullptr;
+    if (k == wcgk) return k32[0];
+    if (k == fvlj4) return k32[1];
+    if (k == kalfs) return k32[2];
+    if (k == vq) return k32[3];
+    return nullptr;
+  }
 
   // k-space kernels [H] and derivative symbols
   double *wcgk = nullptr, *fvlj4 = nullptr, *kalfs = nullptr, *vq = nullptr, *pmod = nullptr;
@@ -221,6 +237,9 @@ int fft_z_only(Handle *h, double2 *buf, bool inverse);
 int fft_x_only(Handle *h, const double *rin, double2 *cout, const double2 *cin, double *rout, bool inverse);
 
 int setup_kernels(Handle *h);
+// element-wise FP64 <-> FP32 conversion of n reals on the handle's stream
+int narrow(Handle *h, const double *in, float *out, size_t n);
+int widen(Handle *h, const float *in, double *out, size_t n);
 
 int field_potenimp(Handle *h);
 int field_poten(Handle *h);

@@ -22,7 +22,7 @@
 #include <cuda_pipeline.h>
 
 #include "common.cuh"
-#include "fft_reg.cuh"
+#include "fft_passes.cuh"
 
 namespace he4 {
 
@@ -222,38 +222,6 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_c2r(XArgs a) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// pencil enumeration for the y and z passes over a half spectrum
-// [nz][ny][nxh].  Pencils are (kx, o) pairs, o = z for the y pass and o = y
-// for the z pass.  Tiles of W pencils with consecutive kx come first; the
-// nxh mod W leftover columns are grouped across o in the last tiles.
-// ---------------------------------------------------------------------------
-struct PencilMap {
-  int nxh, nother, W;
-  long so;  // stride between consecutive o
-};
-
-__device__ __forceinline__ long pencil_offset(const PencilMap &m, long pid, int *kx_out, int *o_out) {
-  const int nfull = m.nxh / m.W;
-  const long main = (long)nfull * m.W * m.nother;
-  const long total = (long)m.nxh * m.nother;
-  if (pid >= total) return -1;
-  int kx, o;
-  if (pid < main) {
-    const long per = (long)nfull * m.W;
-    o = (int)(pid / per);
-    kx = (int)(pid - (long)o * per);
-  } else {
-    const int tw = m.nxh - nfull * m.W;
-    const long r = pid - main;
-    o = (int)(r / tw);
-    kx = nfull * m.W + (int)(r - (long)o * tw);
-  }
-  *kx_out = kx;
-  *o_out = o;
-  return (long)o * m.so + kx;
-}
-
 struct YArgs {
   AxisPlan ay;
   PencilMap map;
@@ -354,6 +322,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_conv(ZArgs a) {
   }
 }
 
+
 // ---------------------------------------------------------------------------
 // twiddle tables
 // ---------------------------------------------------------------------------
@@ -370,13 +339,19 @@ static int axis_init(AxisPlan &A, int n) {
     return HE4_E_UNSUPPORTED;
   }
   double2 *tw = (double2 *)malloc(sizeof(double2) * n);
+  float2 *tw32 = (float2 *)malloc(sizeof(float2) * n);
   for (int t = 0; t < n; t++) {
     long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
-    tw[t] = make_double2((double)cosl(ang), (double)sinl(ang));
+    const long double c = cosl(ang), s = sinl(ang);
+    tw[t] = make_double2((double)c, (double)s);
+    tw32[t] = make_float2((float)c, (float)s);
   }
   cudaError_t e = cudaMalloc(&A.tw, sizeof(double2) * n);
   if (e == cudaSuccess) e = cudaMemcpy(A.tw, tw, sizeof(double2) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&A.tw32, sizeof(float2) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(A.tw32, tw32, sizeof(float2) * n, cudaMemcpyHostToDevice);
   free(tw);
+  free(tw32);
   if (e != cudaSuccess) {
     set_error("twiddle upload: %s", cudaGetErrorString(e));
     return HE4_E_CUDA;
@@ -384,323 +359,12 @@ static int axis_init(AxisPlan &A, int n) {
   return HE4_OK;
 }
 
-
-// ---------------------------------------------------------------------------
-// register-resident passes for power-of-two axes (16..256); see fft_reg.cuh
-// ---------------------------------------------------------------------------
-template <int N>
-struct RegShape;
+template <typename C2>
+static const C2 *twid(const AxisPlan &A);
 template <>
-struct RegShape<16> { static constexpr int N1 = 4; };
+const double2 *twid<double2>(const AxisPlan &A) { return A.tw; }
 template <>
-struct RegShape<32> { static constexpr int N1 = 4; };
-template <>
-struct RegShape<64> { static constexpr int N1 = 8; };
-template <>
-struct RegShape<128> { static constexpr int N1 = 8; };
-template <>
-struct RegShape<256> { static constexpr int N1 = 16; };
-
-static bool reg_ok(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256; }
-
-constexpr int kMaxOut = 6;
-struct ZOut {
-  double2 *out;
-  const double *kern;
-  double coef;
-  int dsym_axis;
-  int boxz;  // store only the z planes of the force box
-};
-struct ZGroup {
-  const double2 *in;
-  int nout;
-  ZOut o[kMaxOut];
-};
-
-struct YRegArgs {
-  PencilMap map;
-  long sf;
-  const double2 *tw;
-  const BoxPair *box;  // non-null: only pencils whose z lies in the force box
-  int nz;
-  double2 *buf[kMaxBatch];
-};
-
-struct ZRegArgs {
-  PencilMap map;
-  long sf;
-  int nx, ny, nz;
-  const double *dsym;
-  const double2 *tw;
-  const BoxPair *box;  // for outputs with boxz
-  ZGroup g[kMaxBatch];
-};
-
-struct XRegArgs {
-  int nxh;
-  long nrow;
-  double scale;
-  const double2 *tw;
-  const BoxPair *box;  // non-null (C2R): only rows (y, z) inside the force box
-  int ny, nz;
-  const double *rin[kMaxBatch];
-  double2 *cout[kMaxBatch];
-  const double2 *cin[kMaxBatch];
-  double *rout[kMaxBatch];
-};
-
-template <int N>
-__device__ __forceinline__ void load_tw_n(double2 *s_tw, const double2 *__restrict__ g_tw) {
-  for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = g_tw[t];
-}
-
-template <int N>
-static size_t smem_yz_reg() {
-  constexpr int N1 = RegShape<N>::N1, W = kThreads / N1;
-  return sizeof(double2) * ((size_t)N * W + N) + (sizeof(long) + 2 * sizeof(int)) * W;
-}
-template <int N>
-static size_t smem_x_reg() {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kThreads / N1;
-  return sizeof(double2) * ((size_t)P * N2 * (N1 + 1) + N);
-}
-
-// in-place transform of strided pencils (y pass, or z without multiply)
-template <int N, bool INV>
-__global__ void __launch_bounds__(kThreads) k_yz_reg(YRegArgs a) {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kThreads / N1;
-  extern __shared__ double2 smem[];
-  double2 *S = smem, *tw = smem + N * W;
-  long *offs = reinterpret_cast<long *>(tw + N);
-  load_tw_n<N>(tw, a.tw);
-  __shared__ int any;
-  if (threadIdx.x == 0) any = 0;
-  __syncthreads();
-  if (threadIdx.x < W) {
-    int kx, o;
-    long of = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
-    if (a.box && of >= 0) {  // pencils along y at plane z = o
-      int lo, hi;
-      force_range(a.box, 2, a.nz, &lo, &hi);
-      if (o < lo || o > hi) of = -1;
-    }
-    offs[threadIdx.x] = of;
-    if (of >= 0) any = 1;
-  }
-  __syncthreads();
-  if (!any) return;
-  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
-  const long off = offs[w];
-  double2 *data = a.buf[blockIdx.y];
-  double2 v[N2];
-#pragma unroll
-  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? data[off + (j1 + N1 * j2) * a.sf] : make_double2(0.0, 0.0);
-  regfft::LayoutYZ lay{W, w};
-  regfft::fwd2<N, N1, INV>(v, S, lay, j1, tw);
-  if (off < 0) return;
-#pragma unroll
-  for (int c = 0; c < N2 / N1; c++)
-#pragma unroll
-    for (int k1 = 0; k1 < N1; k1++) data[off + ((j1 + N1 * c) + N2 * k1) * a.sf] = v[c * N1 + k1];
-}
-
-// z pass: one input per group, FFT_z once, then for each output
-// IFFT_z(coef * K(k) [* i D(k)] * X).  The kernel values K of an output are
-// copied to shared memory with cp.async one output ahead (the first ones
-// before the input is even loaded), so their latency hides behind the FFT
-// work.  SINGLE: one output, multiplied in place (fewer registers).
-template <int N, bool SINGLE>
-static size_t smem_zconv() {
-  constexpr int N1 = RegShape<N>::N1, W = kThreads / N1;
-  return sizeof(double2) * ((size_t)N * W + N) + sizeof(double) * (SINGLE ? 1 : 2) * (size_t)N * W +
-         (sizeof(long) + 2 * sizeof(int)) * W;
-}
-
-template <int N, bool SINGLE>
-__global__ void __launch_bounds__(kThreads) k_zconv_reg(ZRegArgs a) {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kThreads / N1;
-  extern __shared__ double2 smem[];
-  double2 *S = smem, *tw = smem + N * W;
-  double *Ks = reinterpret_cast<double *>(tw + N);  // [SINGLE ? 1 : 2][N][W]
-  long *offs = reinterpret_cast<long *>(Ks + (SINGLE ? 1 : 2) * N * W);
-  int *kxs = reinterpret_cast<int *>(offs + W);
-  int *kys = kxs + W;
-  load_tw_n<N>(tw, a.tw);
-  if (threadIdx.x < W) {
-    int kx = 0, o = 0;
-    offs[threadIdx.x] = pencil_offset(a.map, (long)blockIdx.y * W + threadIdx.x, &kx, &o);
-    kxs[threadIdx.x] = kx;
-    kys[threadIdx.x] = o;
-  }
-  __syncthreads();
-  const ZGroup &G = a.g[blockIdx.x];
-  const int nout = SINGLE ? 1 : G.nout;
-  auto prefetch = [&](int o) {
-    const double *kern = G.o[o].kern;
-    if (!kern) return;
-    double *dst = Ks + (SINGLE ? 0 : (o & 1)) * N * W;
-    for (int e = threadIdx.x; e < N * W; e += kThreads) {
-      const int ww = e % W, k = e / W;
-      const long of = offs[ww];
-      if (of >= 0) __pipeline_memcpy_async(dst + e, kern + of + (long)k * a.sf, sizeof(double));
-    }
-  };
-  prefetch(0);
-  __pipeline_commit();
-  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
-  const long off = offs[w];
-  double2 v[N2];
-#pragma unroll
-  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? G.in[off + (j1 + N1 * j2) * a.sf] : make_double2(0.0, 0.0);
-  regfft::LayoutYZ lay{W, w};
-  regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
-  const double dx = (off >= 0) ? a.dsym[kxs[w]] : 0.0;
-  const double dy = (off >= 0) ? a.dsym[a.nx + kys[w]] : 0.0;
-  for (int o = 0; o < nout; o++) {
-    if (!SINGLE && o + 1 < nout) prefetch(o + 1);
-    __pipeline_commit();
-    __pipeline_wait_prior(1);
-    __syncthreads();
-    const ZOut Z = G.o[o];
-    const double *K = Ks + (SINGLE ? 0 : (o & 1)) * N * W;
-    double2 u[SINGLE ? 1 : N2];
-    double2 *x = SINGLE ? v : u;
-#pragma unroll
-    for (int c = 0; c < N2 / N1; c++)
-#pragma unroll
-      for (int k1 = 0; k1 < N1; k1++) {
-        const int k = (j1 + N1 * c) + N2 * k1;
-        double cf = Z.coef;
-        if (Z.kern && off >= 0) cf *= K[k * W + w];
-        double2 y = cscale(v[c * N1 + k1], cf);
-        if (Z.dsym_axis >= 0) {
-          const double ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
-          y = make_double2(-y.y * ds, y.x * ds);
-        }
-        x[c * N1 + k1] = y;
-      }
-    regfft::bwd2<N, N1, true>(*reinterpret_cast<double2(*)[N2]>(x), S, lay, j1, tw);
-    if (off >= 0) {
-      int zlo = 0, zhi = N - 1;
-      if (Z.boxz) force_range(a.box, 2, a.nz, &zlo, &zhi);
-#pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) {
-        const int z = j1 + N1 * n2;
-        if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
-      }
-    }
-  }
-}
-
-// x pass R2C: two real rows per complex pencil, Hermitian split
-template <int N>
-__global__ void __launch_bounds__(kThreads) k_xr2c_reg(XRegArgs a) {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kThreads / N1, SP = N2 * (N1 + 1);
-  extern __shared__ double2 smem[];
-  double2 *S = smem, *tw = smem + P * SP;
-  load_tw_n<N>(tw, a.tw);
-  __syncthreads();
-  const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
-  const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
-  const double *in = a.rin[blockIdx.y];
-  double2 *out = a.cout[blockIdx.y];
-  double2 v[N2];
-#pragma unroll
-  for (int j2 = 0; j2 < N2; j2++) {
-    const int x = j1 + N1 * j2;
-    v[j2] = make_double2((ra < a.nrow) ? in[ra * N + x] : 0.0, (rb < a.nrow) ? in[rb * N + x] : 0.0);
-  }
-  regfft::LayoutX lay{p * SP};
-  regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
-  double2 *Sp = S + p * SP;
-#pragma unroll
-  for (int c = 0; c < N2 / N1; c++)
-#pragma unroll
-    for (int k1 = 0; k1 < N1; k1++) Sp[(j1 + N1 * c) + N2 * k1] = v[c * N1 + k1];
-  __syncthreads();
-  for (int k = j1; k <= N / 2; k += N1) {
-    const double2 zk = Sp[k];
-    const double2 zm = cconj(Sp[(N - k) & (N - 1)]);
-    const double2 A = cscale(cadd(zk, zm), 0.5);
-    const double2 d = cscale(csub(zk, zm), 0.5);
-    if (ra < a.nrow) out[ra * a.nxh + k] = A;
-    if (rb < a.nrow) out[rb * a.nxh + k] = make_double2(d.y, -d.x);
-  }
-}
-
-// x pass C2R: Hermitian extension of two half spectra, inverse, two rows
-template <int N>
-__global__ void __launch_bounds__(kThreads) k_xc2r_reg(XRegArgs a) {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kThreads / N1, SP = N2 * (N1 + 1);
-  extern __shared__ double2 smem[];
-  double2 *S = smem, *tw = smem + P * SP;
-  load_tw_n<N>(tw, a.tw);
-  const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
-  const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
-  // rows outside the force box (when restricted) are neither read nor written
-  bool ina = ra < a.nrow, inb = rb < a.nrow;
-  if (a.box) {
-    int ylo, yhi, zlo, zhi;
-    force_range(a.box, 1, a.ny, &ylo, &yhi);
-    force_range(a.box, 2, a.nz, &zlo, &zhi);
-    const int ya = (int)(ra % a.ny), za = (int)(ra / a.ny), yb = (int)(rb % a.ny), zb = (int)(rb / a.ny);
-    ina = ina && ya >= ylo && ya <= yhi && za >= zlo && za <= zhi;
-    inb = inb && yb >= ylo && yb <= yhi && zb >= zlo && zb <= zhi;
-    if (!__syncthreads_or(ina || inb)) return;
-  }
-  const double2 *in = a.cin[blockIdx.y];
-  double *out = a.rout[blockIdx.y];
-  double2 *Sp = S + p * SP;
-  for (int k = j1; k < a.nxh; k += N1) {
-    double2 X = ina ? in[ra * a.nxh + k] : make_double2(0.0, 0.0);
-    double2 Y = inb ? in[rb * a.nxh + k] : make_double2(0.0, 0.0);
-    if (k == 0 || 2 * k == N) {  // DC / Nyquist of a real transform: drop Im
-      X.y = 0.0;
-      Y.y = 0.0;
-    }
-    Sp[k] = make_double2(X.x - Y.y, X.y + Y.x);
-    if (k > 0 && N - k >= a.nxh) Sp[N - k] = make_double2(X.x + Y.y, Y.x - X.y);
-  }
-  __syncthreads();
-  double2 v[N2];
-#pragma unroll
-  for (int c = 0; c < N2 / N1; c++)
-#pragma unroll
-    for (int k1 = 0; k1 < N1; k1++) v[c * N1 + k1] = Sp[(j1 + N1 * c) + N2 * k1];
-  __syncthreads();
-  regfft::LayoutX lay{p * SP};
-  regfft::bwd2<N, N1, true>(v, S, lay, j1, tw);
-  const double sc = a.scale;
-#pragma unroll
-  for (int n2 = 0; n2 < N2; n2++) {
-    const int x = j1 + N1 * n2;
-    if (ina) out[ra * N + x] = v[n2].x * sc;
-    if (inb) out[rb * N + x] = v[n2].y * sc;
-  }
-}
-
-template <int N>
-static int reg_attrs() {
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz_reg<N>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_zconv<N, true>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_zconv<N, false>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N>()));
-  return HE4_OK;
-}
-
-// run the statement with NN = n (n one of the register-path lengths)
-#define HE4_REG_SWITCH(n, ...)                                  \
-  switch (n) {                                                  \
-    case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
-    case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
-    case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
-    case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
-    default: { constexpr int NN = 256; __VA_ARGS__; } break;    \
-  }
+const float2 *twid<float2>(const AxisPlan &A) { return A.tw32; }
 
 // ---------------------------------------------------------------------------
 // host side
@@ -734,15 +398,56 @@ int fft_plan_init(FftPlan &P, int nx, int ny, int nz) {
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(nz, P.wz)));
   const int ns[3] = {nx, ny, nz};
   for (int n : ns)
-    if (reg_ok(n)) HE4_REG_SWITCH(n, HE4_TRY(reg_attrs<NN>()));
+    if (reg_ok(n)) {
+      HE4_REG_SWITCH(n, HE4_TRY((reg_attrs<NN, double2>())));
+      HE4_REG_SWITCH(n, HE4_TRY((reg_attrs<NN, float2>())));
+    }
   return HE4_OK;
 }
 
 void fft_plan_free(FftPlan &P) {
-  cudaFree(P.ax.tw);
-  cudaFree(P.ay.tw);
-  cudaFree(P.az.tw);
-  P.ax.tw = P.ay.tw = P.az.tw = nullptr;
+  AxisPlan *axes[3] = {&P.ax, &P.ay, &P.az};
+  for (AxisPlan *A : axes) {
+    cudaFree(A->tw);
+    cudaFree(A->tw32);
+    A->tw = nullptr;
+    A->tw32 = nullptr;
+  }
+}
+
+// register-path x pass in the spectrum type C2 (the real grids stay FP64)
+template <typename C2>
+static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *const *cout, double2 *const *cin,
+                      double *const *rout, bool inverse, const BoxPair *box) {
+  const FftPlan &P = h->fft;
+  const long nrow = (long)P.ny * P.nz;
+  XRegArgs<C2> a{};
+  a.nxh = P.nxh;
+  a.nrow = nrow;
+  a.scale = 1.0;
+  a.tw = twid<C2>(P.ax);
+  a.box = inverse ? box : nullptr;
+  a.ny = P.ny;
+  a.nz = P.nz;
+  for (int i = 0; i < nb; i++) {
+    if (inverse) {
+      a.cin[i] = reinterpret_cast<const C2 *>(cin[i]);
+      a.rout[i] = rout[i];
+    } else {
+      a.rin[i] = rin[i];
+      a.cout[i] = reinterpret_cast<C2 *>(cout[i]);
+    }
+  }
+  HE4_REG_SWITCH(P.nx, {
+    constexpr int Pp = kRegThreads / RegShape<NN>::N1;
+    dim3 grid((unsigned)((nrow + 2 * Pp - 1) / (2 * Pp)), nb);
+    if (inverse)
+      k_xc2r_reg<NN, C2><<<grid, kRegThreads, smem_x_reg<NN, C2>(), h->stream>>>(a);
+    else
+      k_xr2c_reg<NN, C2><<<grid, kRegThreads, smem_x_reg<NN, C2>(), h->stream>>>(a);
+  });
+  HE4_LAUNCHED(h);
+  return HE4_OK;
 }
 
 // box (C2R only, register path): restrict to the rows of the force box
@@ -753,55 +458,72 @@ static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *co
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
     const int nb = std::min(kMaxBatch, n - b0);
     if (reg_ok(P.nx)) {
-      XRegArgs a{};
-      a.nxh = P.nxh;
-      a.nrow = nrow;
-      a.scale = 1.0;
-      a.tw = P.ax.tw;
-      a.box = inverse ? box : nullptr;
-      a.ny = P.ny;
-      a.nz = P.nz;
-      for (int i = 0; i < nb; i++) {
-        if (inverse) {
-          a.cin[i] = cin[b0 + i];
-          a.rout[i] = rout[b0 + i];
-        } else {
-          a.rin[i] = rin[b0 + i];
-          a.cout[i] = cout[b0 + i];
-        }
-      }
-      HE4_REG_SWITCH(P.nx, {
-        constexpr int Pp = kThreads / RegShape<NN>::N1;
-        dim3 grid((unsigned)((nrow + 2 * Pp - 1) / (2 * Pp)), nb);
-        if (inverse)
-          k_xc2r_reg<NN><<<grid, kThreads, smem_x_reg<NN>(), h->stream>>>(a);
-        else
-          k_xr2c_reg<NN><<<grid, kThreads, smem_x_reg<NN>(), h->stream>>>(a);
-      });
-    } else {
-      XArgs a{};
-      a.ax = P.ax;
-      a.nxh = P.nxh;
-      a.P = P.px;
-      a.nrow = nrow;
-      a.scale = 1.0;
-      for (int i = 0; i < nb; i++) {
-        if (inverse) {
-          a.cin[i] = cin[b0 + i];
-          a.rout[i] = rout[b0 + i];
-        } else {
-          a.rin[i] = rin[b0 + i];
-          a.cout[i] = cout[b0 + i];
-        }
-      }
-      dim3 grid((unsigned)((nrow + 2 * P.px - 1) / (2 * P.px)), nb);
-      if (inverse)
-        k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+      const double *const *ri = rin ? rin + b0 : nullptr;
+      double2 *const *co = cout ? cout + b0 : nullptr;
+      double2 *const *ci = cin ? cin + b0 : nullptr;
+      double *const *ro = rout ? rout + b0 : nullptr;
+      if (h->fp32)
+        HE4_TRY(x_pass_reg<float2>(h, nb, ri, co, ci, ro, inverse, box));
       else
-        k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+        HE4_TRY(x_pass_reg<double2>(h, nb, ri, co, ci, ro, inverse, box));
+      continue;
     }
+    if (h->fp32) {
+      set_error("FP32 spectra need register-path axis lengths");
+      return HE4_E_UNSUPPORTED;
+    }
+    XArgs a{};
+    a.ax = P.ax;
+    a.nxh = P.nxh;
+    a.P = P.px;
+    a.nrow = nrow;
+    a.scale = 1.0;
+    for (int i = 0; i < nb; i++) {
+      if (inverse) {
+        a.cin[i] = cin[b0 + i];
+        a.rout[i] = rout[b0 + i];
+      } else {
+        a.rin[i] = rin[b0 + i];
+        a.cout[i] = cout[b0 + i];
+      }
+    }
+    dim3 grid((unsigned)((nrow + 2 * P.px - 1) / (2 * P.px)), nb);
+    if (inverse)
+      k_fft_x_c2r<<<grid, kThreads, smem_x(P), h->stream>>>(a);
+    else
+      k_fft_x_r2c<<<grid, kThreads, smem_x(P), h->stream>>>(a);
     HE4_LAUNCHED(h);
   }
+  return HE4_OK;
+}
+
+// register-path transform of strided pencils in the spectrum type C2
+template <typename C2>
+static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse, const BoxPair *box) {
+  const FftPlan &P = h->fft;
+  const int len = (axis == 1) ? P.ny : P.nz;
+  PencilMap map;
+  map.nxh = P.nxh;
+  map.nother = (axis == 1) ? P.nz : P.ny;
+  map.so = (axis == 1) ? (long)P.ny * P.nxh : P.nxh;
+  const long total = (long)P.nxh * map.nother;
+  YRegArgs<C2> a{};
+  a.sf = (axis == 1) ? (long)P.nxh : (long)P.ny * P.nxh;
+  a.tw = twid<C2>((axis == 1) ? P.ay : P.az);
+  a.box = (axis == 1) ? box : nullptr;
+  a.nz = P.nz;
+  for (int i = 0; i < nb; i++) a.buf[i] = reinterpret_cast<C2 *>(buf[i]);
+  HE4_REG_SWITCH(len, {
+    constexpr int W = kRegThreads / RegShape<NN>::N1;
+    map.W = W;
+    a.map = map;
+    dim3 grid((unsigned)((total + W - 1) / W), nb);
+    if (inverse)
+      k_yz_reg<NN, true, C2><<<grid, kRegThreads, smem_yz_reg<NN, C2>(), h->stream>>>(a);
+    else
+      k_yz_reg<NN, false, C2><<<grid, kRegThreads, smem_yz_reg<NN, C2>(), h->stream>>>(a);
+  });
+  HE4_LAUNCHED(h);
   return HE4_OK;
 }
 
@@ -811,34 +533,26 @@ static int strided_pass(Handle *h, int n, double2 *const *buf, int axis, bool in
                         const BoxPair *box = nullptr) {
   const FftPlan &P = h->fft;
   const int len = (axis == 1) ? P.ny : P.nz;
-  const AxisPlan &A = (axis == 1) ? P.ay : P.az;
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
     const int nb = std::min(kMaxBatch, n - b0);
+    if (reg_ok(len)) {
+      if (h->fp32)
+        HE4_TRY(yz_reg<float2>(h, nb, buf + b0, axis, inverse, box));
+      else
+        HE4_TRY(yz_reg<double2>(h, nb, buf + b0, axis, inverse, box));
+      continue;
+    }
+    if (h->fp32) {
+      set_error("FP32 spectra need register-path axis lengths");
+      return HE4_E_UNSUPPORTED;
+    }
     PencilMap map;
     map.nxh = P.nxh;
     map.nother = (axis == 1) ? P.nz : P.ny;
     map.so = (axis == 1) ? (long)P.ny * P.nxh : P.nxh;
     const long sf = (axis == 1) ? (long)P.nxh : (long)P.ny * P.nxh;
     const long total = (long)P.nxh * map.nother;
-    if (reg_ok(len)) {
-      YRegArgs a{};
-      a.sf = sf;
-      a.tw = A.tw;
-      a.box = (axis == 1) ? box : nullptr;
-      a.nz = P.nz;
-      for (int i = 0; i < nb; i++) a.buf[i] = buf[b0 + i];
-      HE4_REG_SWITCH(len, {
-        constexpr int W = kThreads / RegShape<NN>::N1;
-        map.W = W;
-        a.map = map;
-        dim3 grid((unsigned)((total + W - 1) / W), nb);
-        if (inverse)
-          k_yz_reg<NN, true><<<grid, kThreads, smem_yz_reg<NN>(), h->stream>>>(a);
-        else
-          k_yz_reg<NN, false><<<grid, kThreads, smem_yz_reg<NN>(), h->stream>>>(a);
-      });
-      HE4_LAUNCHED(h);
-    } else if (axis == 1) {
+    if (axis == 1) {
       YArgs a{};
       a.ay = P.ay;
       map.W = P.wy;
@@ -881,53 +595,83 @@ int fft_c2r_box(Handle *h, int n, double2 *const *in, double *const *out) {
   return HE4_OK;
 }
 
+// kernel array of an operation in the spectrum type's real type
+template <typename C2>
+static const typename regfft::Re<C2>::type *kern_of(const Handle *h, const double *k);
+template <>
+const double *kern_of<double2>(const Handle *, const double *k) { return k; }
+template <>
+const float *kern_of<float2>(const Handle *h, const double *k) { return h->kern32(k); }
+
+template <typename C2>
+static const typename regfft::Re<C2>::type *dsym_of(const Handle *h);
+template <>
+const double *dsym_of<double2>(const Handle *h) { return h->dsym; }
+template <>
+const float *dsym_of<float2>(const Handle *h) { return h->dsym32; }
+
+// register-path fused z pass: consecutive operations on the same input share
+// one forward transform
+template <typename C2>
+static int zconv_reg(Handle *h, int n, const ZOp *ops) {
+  const FftPlan &P = h->fft;
+  ZGroupT<C2> groups[64];
+  int ng = 0;
+  for (int i = 0; i < n; i++) {
+    const C2 *in = reinterpret_cast<const C2 *>(ops[i].in);
+    if (ng == 0 || groups[ng - 1].in != in || groups[ng - 1].nout == kMaxOut) {
+      if (ng == 64) {
+        set_error("too many z-pass groups");
+        return HE4_E_ARG;
+      }
+      groups[ng].in = in;
+      groups[ng].nout = 0;
+      ng++;
+    }
+    if (ops[i].kern && !kern_of<C2>(h, ops[i].kern)) {
+      set_error("no FP32 copy of a z-pass kernel");
+      return HE4_E_ARG;
+    }
+    ZGroupT<C2> &g = groups[ng - 1];
+    g.o[g.nout++] = ZOutT<C2>{reinterpret_cast<C2 *>(ops[i].out), kern_of<C2>(h, ops[i].kern), ops[i].coef,
+                              ops[i].dsym_axis, ops[i].boxz};
+  }
+  for (int g0 = 0; g0 < ng; g0 += kMaxBatch) {
+    const int nb = std::min(kMaxBatch, ng - g0);
+    ZRegArgs<C2> a{};
+    a.map.nxh = P.nxh;
+    a.map.nother = P.ny;
+    a.map.so = P.nxh;
+    a.sf = (long)P.ny * P.nxh;
+    a.nx = P.nx;
+    a.ny = P.ny;
+    a.nz = P.nz;
+    a.dsym = dsym_of<C2>(h);
+    a.tw = twid<C2>(P.az);
+    a.box = h->box;
+    for (int i = 0; i < nb; i++) a.g[i] = groups[g0 + i];
+    const long total = (long)P.nxh * P.ny;
+    bool single = true;
+    for (int i = 0; i < nb; i++) single = single && (a.g[i].nout == 1);
+    HE4_REG_SWITCH(P.nz, {
+      constexpr int W = kRegThreads / RegShape<NN>::N1;
+      a.map.W = W;
+      dim3 grid(nb, (unsigned)((total + W - 1) / W));
+      if (single)
+        k_zconv_reg<NN, true, C2><<<grid, kRegThreads, smem_zconv<NN, true, C2>(), h->stream>>>(a);
+      else
+        k_zconv_reg<NN, false, C2><<<grid, kRegThreads, smem_zconv<NN, false, C2>(), h->stream>>>(a);
+    });
+    HE4_LAUNCHED(h);
+  }
+  return HE4_OK;
+}
+
 int fft_z_conv(Handle *h, int n, const ZOp *ops) {
   const FftPlan &P = h->fft;
   if (n <= 0) return HE4_OK;
   const bool plain = ops[0].mode != 0;
-  if (reg_ok(P.nz) && !plain) {
-    // group consecutive operations that read the same input
-    ZGroup groups[64];
-    int ng = 0;
-    for (int i = 0; i < n; i++) {
-      if (ng == 0 || groups[ng - 1].in != ops[i].in || groups[ng - 1].nout == kMaxOut) {
-        groups[ng].in = ops[i].in;
-        groups[ng].nout = 0;
-        ng++;
-      }
-      ZGroup &g = groups[ng - 1];
-      g.o[g.nout++] = ZOut{ops[i].out, ops[i].kern, ops[i].coef, ops[i].dsym_axis, ops[i].boxz};
-    }
-    for (int g0 = 0; g0 < ng; g0 += kMaxBatch) {
-      const int nb = std::min(kMaxBatch, ng - g0);
-      ZRegArgs a{};
-      a.map.nxh = P.nxh;
-      a.map.nother = P.ny;
-      a.map.so = P.nxh;
-      a.sf = (long)P.ny * P.nxh;
-      a.nx = P.nx;
-      a.ny = P.ny;
-      a.nz = P.nz;
-      a.dsym = h->dsym;
-      a.tw = P.az.tw;
-      a.box = h->box;
-      for (int i = 0; i < nb; i++) a.g[i] = groups[g0 + i];
-      const long total = (long)P.nxh * P.ny;
-      bool single = true;
-      for (int i = 0; i < nb; i++) single = single && (a.g[i].nout == 1);
-      HE4_REG_SWITCH(P.nz, {
-        constexpr int W = kThreads / RegShape<NN>::N1;
-        a.map.W = W;
-        dim3 grid(nb, (unsigned)((total + W - 1) / W));
-        if (single)
-          k_zconv_reg<NN, true><<<grid, kThreads, smem_zconv<NN, true>(), h->stream>>>(a);
-        else
-          k_zconv_reg<NN, false><<<grid, kThreads, smem_zconv<NN, false>(), h->stream>>>(a);
-      });
-      HE4_LAUNCHED(h);
-    }
-    return HE4_OK;
-  }
+  if (reg_ok(P.nz) && !plain) return h->fp32 ? zconv_reg<float2>(h, n, ops) : zconv_reg<double2>(h, n, ops);
   if (reg_ok(P.nz) && plain) {
     for (int i = 0; i < n; i++) {
       double2 *b[1] = {ops[i].out};
@@ -938,6 +682,10 @@ int fft_z_conv(Handle *h, int n, const ZOp *ops) {
       HE4_TRY(strided_pass(h, 1, b, 2, ops[i].mode == 2));
     }
     return HE4_OK;
+  }
+  if (h->fp32) {
+    set_error("FP32 spectra need register-path axis lengths");
+    return HE4_E_UNSUPPORTED;
   }
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
     int nb = std::min(kMaxBatch, n - b0);

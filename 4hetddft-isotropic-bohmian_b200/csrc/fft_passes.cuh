@@ -1,0 +1,373 @@
+// fft_passes.cuh -- the register-resident x, y and z pass kernels (lengths
+// 16..256, powers of two), templated on the complex type of the spectra:
+// double2 (plain FP64 form) or float2 (FP32-convolution form).  Real grids
+// are FP64 in both forms; the x passes convert on load and store.
+#pragma once
+#include <cuda_pipeline.h>
+
+#include "common.cuh"
+#include "fft_reg.cuh"
+
+namespace he4 {
+
+constexpr int kRegThreads = 256;
+constexpr int kRegBatch = 8;
+
+template <int N>
+struct RegShape;
+template <>
+struct RegShape<16> { static constexpr int N1 = 4; };
+template <>
+struct RegShape<32> { static constexpr int N1 = 4; };
+template <>
+struct RegShape<64> { static constexpr int N1 = 8; };
+template <>
+struct RegShape<128> { static constexpr int N1 = 8; };
+template <>
+struct RegShape<256> { static constexpr int N1 = 16; };
+
+inline bool reg_ok(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256; }
+
+// pencil enumeration for the y and z passes over a half spectrum
+// [nz][ny][nxh].  Pencils are (kx, o) pairs, o = z for the y pass and o = y
+// for the z pass.  Tiles of W pencils with consecutive kx come first; the
+// nxh mod W leftover columns are grouped across o in the last tiles.
+struct PencilMap {
+  int nxh, nother, W;
+  long so;  // stride between consecutive o
+};
+
+__device__ __forceinline__ long pencil_offset(const PencilMap &m, long pid, int *kx_out, int *o_out) {
+  const int nfull = m.nxh / m.W;
+  const long main = (long)nfull * m.W * m.nother;
+  const long total = (long)m.nxh * m.nother;
+  if (pid >= total) return -1;
+  int kx, o;
+  if (pid < main) {
+    const long per = (long)nfull * m.W;
+    o = (int)(pid / per);
+    kx = (int)(pid - (long)o * per);
+  } else {
+    const int tw = m.nxh - nfull * m.W;
+    const long r = pid - main;
+    o = (int)(r / tw);
+    kx = nfull * m.W + (int)(r - (long)o * tw);
+  }
+  *kx_out = kx;
+  *o_out = o;
+  return (long)o * m.so + kx;
+}
+
+constexpr int kMaxOut = 6;
+template <typename C2>
+struct ZOutT {
+  C2 *out;
+  const typename regfft::Re<C2>::type *kern;
+  double coef;
+  int dsym_axis;
+  int boxz;  // store only the z planes of the force box
+};
+template <typename C2>
+struct ZGroupT {
+  const C2 *in;
+  int nout;
+  ZOutT<C2> o[kMaxOut];
+};
+
+template <typename C2>
+struct YRegArgs {
+  PencilMap map;
+  long sf;
+  const C2 *tw;
+  const BoxPair *box;  // non-null: only pencils whose z lies in the force box
+  int nz;
+  C2 *buf[kRegBatch];
+};
+
+template <typename C2>
+struct ZRegArgs {
+  PencilMap map;
+  long sf;
+  int nx, ny, nz;
+  const typename regfft::Re<C2>::type *dsym;
+  const C2 *tw;
+  const BoxPair *box;  // for outputs with boxz
+  ZGroupT<C2> g[kRegBatch];
+};
+
+template <typename C2>
+struct XRegArgs {
+  int nxh;
+  long nrow;
+  double scale;
+  const C2 *tw;
+  const BoxPair *box;  // non-null (C2R): only rows (y, z) inside the force box
+  int ny, nz;
+  const double *rin[kRegBatch];
+  C2 *cout[kRegBatch];
+  const C2 *cin[kRegBatch];
+  double *rout[kRegBatch];
+};
+
+template <int N, typename C2>
+__device__ __forceinline__ void load_tw_n(C2 *s_tw, const C2 *__restrict__ g_tw) {
+  for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = g_tw[t];
+}
+
+template <int N, typename C2>
+inline size_t smem_yz_reg() {
+  constexpr int N1 = RegShape<N>::N1, W = kRegThreads / N1;
+  return sizeof(C2) * ((size_t)N * W + N) + (sizeof(long) + 2 * sizeof(int)) * W;
+}
+template <int N, typename C2>
+inline size_t smem_x_reg() {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kRegThreads / N1;
+  return sizeof(C2) * ((size_t)P * N2 * (N1 + 1) + N);
+}
+template <int N, bool SINGLE, typename C2>
+inline size_t smem_zconv() {
+  using T = typename regfft::Re<C2>::type;
+  constexpr int N1 = RegShape<N>::N1, W = kRegThreads / N1;
+  return sizeof(C2) * ((size_t)N * W + N) + sizeof(T) * (SINGLE ? 1 : 2) * (size_t)N * W +
+         (sizeof(long) + 2 * sizeof(int)) * W;
+}
+
+// in-place transform of strided pencils (y pass, or z without multiply)
+template <int N, bool INV, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_yz_reg(YRegArgs<C2> a) {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kRegThreads / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
+  long *offs = reinterpret_cast<long *>(tw + N);
+  load_tw_n<N>(tw, a.tw);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  if (threadIdx.x < W) {
+    int kx, o;
+    long of = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
+    if (a.box && of >= 0) {  // pencils along y at plane z = o
+      int lo, hi;
+      force_range(a.box, 2, a.nz, &lo, &hi);
+      if (o < lo || o > hi) of = -1;
+    }
+    offs[threadIdx.x] = of;
+    if (of >= 0) any = 1;
+  }
+  __syncthreads();
+  if (!any) return;
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  const long off = offs[w];
+  C2 *data = a.buf[blockIdx.y];
+  C2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? data[off + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+  regfft::LayoutYZ lay{W, w};
+  regfft::fwd2<N, N1, INV>(v, S, lay, j1, tw);
+  if (off < 0) return;
+#pragma unroll
+  for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) data[off + ((j1 + N1 * c) + N2 * k1) * a.sf] = v[c * N1 + k1];
+}
+
+// z pass: one input per group, FFT_z once, then for each output
+// IFFT_z(coef * K(k) [* i D(k)] * X).  The kernel values K of an output are
+// copied to shared memory with cp.async one output ahead (the first ones
+// before the input is even loaded), so their latency hides behind the FFT
+// work.  SINGLE: one output, multiplied in place (fewer registers).
+template <int N, bool SINGLE, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
+  using T = typename regfft::Re<C2>::type;
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kRegThreads / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
+  T *Ks = reinterpret_cast<T *>(tw + N);  // [SINGLE ? 1 : 2][N][W]
+  long *offs = reinterpret_cast<long *>(Ks + (SINGLE ? 1 : 2) * N * W);
+  int *kxs = reinterpret_cast<int *>(offs + W);
+  int *kys = kxs + W;
+  load_tw_n<N>(tw, a.tw);
+  if (threadIdx.x < W) {
+    int kx = 0, o = 0;
+    offs[threadIdx.x] = pencil_offset(a.map, (long)blockIdx.y * W + threadIdx.x, &kx, &o);
+    kxs[threadIdx.x] = kx;
+    kys[threadIdx.x] = o;
+  }
+  __syncthreads();
+  const ZGroupT<C2> &G = a.g[blockIdx.x];
+  const int nout = SINGLE ? 1 : G.nout;
+  auto prefetch = [&](int o) {
+    const T *kern = G.o[o].kern;
+    if (!kern) return;
+    T *dst = Ks + (SINGLE ? 0 : (o & 1)) * N * W;
+    for (int e = threadIdx.x; e < N * W; e += kRegThreads) {
+      const int ww = e % W, k = e / W;
+      const long of = offs[ww];
+      if (of >= 0) __pipeline_memcpy_async(dst + e, kern + of + (long)k * a.sf, sizeof(T));
+    }
+  };
+  prefetch(0);
+  __pipeline_commit();
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  const long off = offs[w];
+  C2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? G.in[off + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+  regfft::LayoutYZ lay{W, w};
+  regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
+  const T dx = (off >= 0) ? a.dsym[kxs[w]] : T(0);
+  const T dy = (off >= 0) ? a.dsym[a.nx + kys[w]] : T(0);
+  for (int o = 0; o < nout; o++) {
+    if (!SINGLE && o + 1 < nout) prefetch(o + 1);
+    __pipeline_commit();
+    __pipeline_wait_prior(1);
+    __syncthreads();
+    const ZOutT<C2> Z = G.o[o];
+    const T *K = Ks + (SINGLE ? 0 : (o & 1)) * N * W;
+    C2 u[SINGLE ? 1 : N2];
+    C2 *x = SINGLE ? v : u;
+    const T coef = (T)Z.coef;
+#pragma unroll
+    for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) {
+        const int k = (j1 + N1 * c) + N2 * k1;
+        T cf = coef;
+        if (Z.kern && off >= 0) cf *= K[k * W + w];
+        C2 y = regfft::scale(v[c * N1 + k1], cf);
+        if (Z.dsym_axis >= 0) {
+          const T ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
+          y = regfft::mk<C2>(-y.y * ds, y.x * ds);
+        }
+        x[c * N1 + k1] = y;
+      }
+    regfft::bwd2<N, N1, true>(*reinterpret_cast<C2(*)[N2]>(x), S, lay, j1, tw);
+    if (off >= 0) {
+      int zlo = 0, zhi = N - 1;
+      if (Z.boxz) force_range(a.box, 2, a.nz, &zlo, &zhi);
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) {
+        const int z = j1 + N1 * n2;
+        if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+      }
+    }
+  }
+}
+
+// x pass R2C: two real rows per complex pencil, Hermitian split
+template <int N, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
+  using T = typename regfft::Re<C2>::type;
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + P * SP;
+  load_tw_n<N>(tw, a.tw);
+  __syncthreads();
+  const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
+  const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
+  const double *in = a.rin[blockIdx.y];
+  C2 *out = a.cout[blockIdx.y];
+  C2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) {
+    const int x = j1 + N1 * j2;
+    v[j2] = regfft::mk<C2>((T)((ra < a.nrow) ? in[ra * N + x] : 0.0), (T)((rb < a.nrow) ? in[rb * N + x] : 0.0));
+  }
+  regfft::LayoutX lay{p * SP};
+  regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
+  C2 *Sp = S + p * SP;
+#pragma unroll
+  for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) Sp[(j1 + N1 * c) + N2 * k1] = v[c * N1 + k1];
+  __syncthreads();
+  for (int k = j1; k <= N / 2; k += N1) {
+    const C2 zk = Sp[k];
+    const C2 zmc = Sp[(N - k) & (N - 1)];
+    const C2 zm = regfft::mk<C2>(zmc.x, -zmc.y);
+    const C2 A = regfft::scale(regfft::add(zk, zm), T(0.5));
+    const C2 d = regfft::scale(regfft::sub(zk, zm), T(0.5));
+    if (ra < a.nrow) out[ra * a.nxh + k] = A;
+    if (rb < a.nrow) out[rb * a.nxh + k] = regfft::mk<C2>(d.y, -d.x);
+  }
+}
+
+// x pass C2R: Hermitian extension of two half spectra, inverse, two rows
+template <int N, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + P * SP;
+  load_tw_n<N>(tw, a.tw);
+  const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
+  const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
+  // rows outside the force box (when restricted) are neither read nor written
+  bool ina = ra < a.nrow, inb = rb < a.nrow;
+  if (a.box) {
+    int ylo, yhi, zlo, zhi;
+    force_range(a.box, 1, a.ny, &ylo, &yhi);
+    force_range(a.box, 2, a.nz, &zlo, &zhi);
+    const int ya = (int)(ra % a.ny), za = (int)(ra / a.ny), yb = (int)(rb % a.ny), zb = (int)(rb / a.ny);
+    ina = ina && ya >= ylo && ya <= yhi && za >= zlo && za <= zhi;
+    inb = inb && yb >= ylo && yb <= yhi && zb >= zlo && zb <= zhi;
+    if (!__syncthreads_or(ina || inb)) return;
+  }
+  const C2 *in = a.cin[blockIdx.y];
+  double *out = a.rout[blockIdx.y];
+  C2 *Sp = S + p * SP;
+  for (int k = j1; k < a.nxh; k += N1) {
+    C2 X = ina ? in[ra * a.nxh + k] : regfft::mk<C2>(0, 0);
+    C2 Y = inb ? in[rb * a.nxh + k] : regfft::mk<C2>(0, 0);
+    if (k == 0 || 2 * k == N) {  // DC / Nyquist of a real transform: drop Im
+      X.y = 0;
+      Y.y = 0;
+    }
+    Sp[k] = regfft::mk<C2>(X.x - Y.y, X.y + Y.x);
+    if (k > 0 && N - k >= a.nxh) Sp[N - k] = regfft::mk<C2>(X.x + Y.y, Y.x - X.y);
+  }
+  __syncthreads();
+  C2 v[N2];
+#pragma unroll
+  for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) v[c * N1 + k1] = Sp[(j1 + N1 * c) + N2 * k1];
+  __syncthreads();
+  regfft::LayoutX lay{p * SP};
+  regfft::bwd2<N, N1, true>(v, S, lay, j1, tw);
+  const double sc = a.scale;
+#pragma unroll
+  for (int n2 = 0; n2 < N2; n2++) {
+    const int x = j1 + N1 * n2;
+    if (ina) out[ra * N + x] = (double)v[n2].x * sc;
+    if (inb) out[rb * N + x] = (double)v[n2].y * sc;
+  }
+}
+
+template <int N, typename C2>
+inline int reg_attrs() {
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_yz_reg<N, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_yz_reg<N, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zconv<N, true, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zconv<N, false, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_x_reg<N, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_x_reg<N, C2>()));
+  return HE4_OK;
+}
+
+// run the statement with NN = n (n one of the register-path lengths)
+#define HE4_REG_SWITCH(n, ...)                                  \
+  switch (n) {                                                  \
+    case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
+    case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
+    case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
+    case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
+    default: { constexpr int NN = 256; __VA_ARGS__; } break;    \
+  }
+
+}  // namespace he4

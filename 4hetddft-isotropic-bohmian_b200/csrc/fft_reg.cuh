@@ -1,5 +1,6 @@
 // fft_reg.cuh -- register-resident pencil FFTs for lengths 16..256 (powers
-// of two), used by the x, y and z passes when the axis length allows.
+// of two), used by the x, y and z passes when the axis length allows, in
+// FP64 (double2) or FP32 (float2).
 //
 // A length-N transform is split N = N1 * N2 (four-step form).  With
 // j = j1 + N1 j2 and k = k2 + N2 k1:
@@ -17,97 +18,138 @@
 namespace he4 {
 namespace regfft {
 
+// complex type of a real type
+template <typename T>
+struct Cx;
+template <>
+struct Cx<double> {
+  using type = double2;
+};
+template <>
+struct Cx<float> {
+  using type = float2;
+};
+
+template <typename C2>
+struct Re;
+template <>
+struct Re<double2> {
+  using type = double;
+};
+template <>
+struct Re<float2> {
+  using type = float;
+};
+
+template <typename C2>
+__device__ __forceinline__ C2 mk(typename Re<C2>::type a, typename Re<C2>::type b) {
+  C2 r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <typename C2>
+__device__ __forceinline__ C2 add(C2 a, C2 b) { return mk<C2>(a.x + b.x, a.y + b.y); }
+template <typename C2>
+__device__ __forceinline__ C2 sub(C2 a, C2 b) { return mk<C2>(a.x - b.x, a.y - b.y); }
+template <typename C2>
+__device__ __forceinline__ C2 scale(C2 a, typename Re<C2>::type s) { return mk<C2>(a.x * s, a.y * s); }
+template <typename C2>
+__device__ __forceinline__ C2 mul(C2 a, C2 b) { return mk<C2>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
 constexpr double kR2 = 0.70710678118654752440;   // cos(pi/4)
 constexpr double kC1 = 0.92387953251128675613;   // cos(pi/8)
 constexpr double kS1 = 0.38268343236508977173;   // sin(pi/8)
 
 // v * w_16^m for compile-time m (forward root exp(-2 pi i m / 16))
-template <int M, bool INV>
-__device__ __forceinline__ double2 rot16(double2 v) {
+template <int M, bool INV, typename C2>
+__device__ __forceinline__ C2 rot16(C2 v) {
+  using T = typename Re<C2>::type;
   constexpr int m = M & 15;
   if (m == 0) return v;
-  if (m == 4) return INV ? make_double2(-v.y, v.x) : make_double2(v.y, -v.x);
-  if (m == 8) return make_double2(-v.x, -v.y);
-  if (m == 12) return INV ? make_double2(v.y, -v.x) : make_double2(-v.y, v.x);
-  double c, s;
+  if (m == 4) return INV ? mk<C2>(-v.y, v.x) : mk<C2>(v.y, -v.x);
+  if (m == 8) return mk<C2>(-v.x, -v.y);
+  if (m == 12) return INV ? mk<C2>(v.y, -v.x) : mk<C2>(-v.y, v.x);
+  double cd, sd;
   switch (m) {
-    case 1: c = kC1; s = kS1; break;
-    case 2: c = kR2; s = kR2; break;
-    case 3: c = kS1; s = kC1; break;
-    case 5: c = -kS1; s = kC1; break;
-    case 6: c = -kR2; s = kR2; break;
-    case 7: c = -kC1; s = kS1; break;
-    case 9: c = -kC1; s = -kS1; break;
-    case 10: c = -kR2; s = -kR2; break;
-    case 11: c = -kS1; s = -kC1; break;
-    case 13: c = kS1; s = -kC1; break;
-    case 14: c = kR2; s = -kR2; break;
-    default: c = kC1; s = -kS1; break;  // 15
+    case 1: cd = kC1; sd = kS1; break;
+    case 2: cd = kR2; sd = kR2; break;
+    case 3: cd = kS1; sd = kC1; break;
+    case 5: cd = -kS1; sd = kC1; break;
+    case 6: cd = -kR2; sd = kR2; break;
+    case 7: cd = -kC1; sd = kS1; break;
+    case 9: cd = -kC1; sd = -kS1; break;
+    case 10: cd = -kR2; sd = -kR2; break;
+    case 11: cd = -kS1; sd = -kC1; break;
+    case 13: cd = kS1; sd = -kC1; break;
+    case 14: cd = kR2; sd = -kR2; break;
+    default: cd = kC1; sd = -kS1; break;  // 15
   }
+  const T c = (T)cd, s = (T)sd;
   // forward root: c - i s ; inverse: c + i s
-  if (INV) return make_double2(v.x * c - v.y * s, v.x * s + v.y * c);
-  return make_double2(v.x * c + v.y * s, v.y * c - v.x * s);
+  if (INV) return mk<C2>(v.x * c - v.y * s, v.x * s + v.y * c);
+  return mk<C2>(v.x * c + v.y * s, v.y * c - v.x * s);
 }
 
-template <bool INV>
-__device__ __forceinline__ double2 muli(double2 a) {  // -i a (fwd), +i a (inv)
-  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <bool INV, typename C2>
+__device__ __forceinline__ C2 muli(C2 a) {  // -i a (fwd), +i a (inv)
+  return INV ? mk<C2>(-a.y, a.x) : mk<C2>(a.y, -a.x);
 }
 
-template <bool INV>
-__device__ __forceinline__ void dft4(double2 &x0, double2 &x1, double2 &x2, double2 &x3) {
-  const double2 a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = muli<INV>(csub(x1, x3));
-  x0 = cadd(a, c);
-  x2 = csub(a, c);
-  x1 = cadd(b, d);
-  x3 = csub(b, d);
+template <bool INV, typename C2>
+__device__ __forceinline__ void dft4(C2 &x0, C2 &x1, C2 &x2, C2 &x3) {
+  const C2 a = add(x0, x2), b = sub(x0, x2), c = add(x1, x3), d = muli<INV>(sub(x1, x3));
+  x0 = add(a, c);
+  x2 = sub(a, c);
+  x1 = add(b, d);
+  x3 = sub(b, d);
 }
 
 // in-place DFT of R points held in v[0..R-1] (natural order in and out)
-template <int R, bool INV>
+template <int R, bool INV, typename C2>
 struct Dft;
 
-template <bool INV>
-struct Dft<2, INV> {
-  static __device__ __forceinline__ void run(double2 *v) {
-    const double2 t = v[0];
-    v[0] = cadd(t, v[1]);
-    v[1] = csub(t, v[1]);
+template <bool INV, typename C2>
+struct Dft<2, INV, C2> {
+  static __device__ __forceinline__ void run(C2 *v) {
+    const C2 t = v[0];
+    v[0] = add(t, v[1]);
+    v[1] = sub(t, v[1]);
   }
 };
 
-template <bool INV>
-struct Dft<4, INV> {
-  static __device__ __forceinline__ void run(double2 *v) { dft4<INV>(v[0], v[1], v[2], v[3]); }
+template <bool INV, typename C2>
+struct Dft<4, INV, C2> {
+  static __device__ __forceinline__ void run(C2 *v) { dft4<INV>(v[0], v[1], v[2], v[3]); }
 };
 
-template <bool INV>
-struct Dft<8, INV> {
+template <bool INV, typename C2>
+struct Dft<8, INV, C2> {
   // j = j1 + 2 j2: DFT4 over j2 for j1 = 0, 1; twiddle w_8^(j1 k2); DFT2
-  static __device__ __forceinline__ void run(double2 *v) {
-    double2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
-    double2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
+  static __device__ __forceinline__ void run(C2 *v) {
+    C2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
+    C2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
     dft4<INV>(a0, a1, a2, a3);
     dft4<INV>(b0, b1, b2, b3);
     b1 = rot16<2, INV>(b1);
     b2 = rot16<4, INV>(b2);
     b3 = rot16<6, INV>(b3);
-    v[0] = cadd(a0, b0);
-    v[4] = csub(a0, b0);
-    v[1] = cadd(a1, b1);
-    v[5] = csub(a1, b1);
-    v[2] = cadd(a2, b2);
-    v[6] = csub(a2, b2);
-    v[3] = cadd(a3, b3);
-    v[7] = csub(a3, b3);
+    v[0] = add(a0, b0);
+    v[4] = sub(a0, b0);
+    v[1] = add(a1, b1);
+    v[5] = sub(a1, b1);
+    v[2] = add(a2, b2);
+    v[6] = sub(a2, b2);
+    v[3] = add(a3, b3);
+    v[7] = sub(a3, b3);
   }
 };
 
-template <bool INV>
-struct Dft<16, INV> {
+template <bool INV, typename C2>
+struct Dft<16, INV, C2> {
   // j = j1 + 4 j2: DFT4 over j2 for each j1; twiddle w_16^(j1 k2); DFT4 over j1
-  static __device__ __forceinline__ void run(double2 *v) {
-    double2 y[4][4];
+  static __device__ __forceinline__ void run(C2 *v) {
+    C2 y[4][4];
 #pragma unroll
     for (int j1 = 0; j1 < 4; j1++) {
       y[j1][0] = v[j1];
@@ -127,7 +169,7 @@ struct Dft<16, INV> {
     y[3][3] = rot16<9, INV>(y[3][3]);
 #pragma unroll
     for (int k2 = 0; k2 < 4; k2++) {
-      double2 a = y[0][k2], b = y[1][k2], c = y[2][k2], d = y[3][k2];
+      C2 a = y[0][k2], b = y[1][k2], c = y[2][k2], d = y[3][k2];
       dft4<INV>(a, b, c, d);
       v[k2] = a;
       v[k2 + 4] = b;
@@ -151,17 +193,16 @@ struct LayoutX {
 };
 
 // forward: a[j2] = x[j1 + N1 j2]  ->  a[c N1 + k1] = X[(q + N1 c) + N2 k1], q = j1
-template <int N, int N1, bool INV, typename L>
-__device__ __forceinline__ void fwd2(double2 (&a)[N / N1], double2 *S, const L &lay, int j1,
-                                     const double2 *__restrict__ tw) {
+template <int N, int N1, bool INV, typename L, typename C2>
+__device__ __forceinline__ void fwd2(C2 (&a)[N / N1], C2 *S, const L &lay, int j1, const C2 *__restrict__ tw) {
   constexpr int N2 = N / N1;
   static_assert(N2 % N1 == 0, "N2 must be a multiple of N1");
-  Dft<N2, INV>::run(a);
+  Dft<N2, INV, C2>::run(a);
 #pragma unroll
   for (int k2 = 1; k2 < N2; k2++) {
-    double2 t = tw[j1 * k2];
+    C2 t = tw[j1 * k2];
     if (INV) t.y = -t.y;
-    a[k2] = cmul(a[k2], t);
+    a[k2] = mul(a[k2], t);
   }
 #pragma unroll
   for (int k2 = 0; k2 < N2; k2++) S[lay.at(k2, j1, N1)] = a[k2];
@@ -169,10 +210,10 @@ __device__ __forceinline__ void fwd2(double2 (&a)[N / N1], double2 *S, const L &
 #pragma unroll
   for (int c = 0; c < N2 / N1; c++) {
     const int k2 = j1 + N1 * c;
-    double2 b[N1];
+    C2 b[N1];
 #pragma unroll
     for (int jj = 0; jj < N1; jj++) b[jj] = S[lay.at(k2, jj, N1)];
-    Dft<N1, INV>::run(b);
+    Dft<N1, INV, C2>::run(b);
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) a[c * N1 + k1] = b[k1];
   }
@@ -181,28 +222,27 @@ __device__ __forceinline__ void fwd2(double2 (&a)[N / N1], double2 *S, const L &
 
 // inverse of fwd2's layout: a[c N1 + k1] = X[(q + N1 c) + N2 k1]  ->
 // a[n2] = x[j1 + N1 n2] (unnormalised; INV selects the root direction)
-template <int N, int N1, bool INV, typename L>
-__device__ __forceinline__ void bwd2(double2 (&a)[N / N1], double2 *S, const L &lay, int j1,
-                                     const double2 *__restrict__ tw) {
+template <int N, int N1, bool INV, typename L, typename C2>
+__device__ __forceinline__ void bwd2(C2 (&a)[N / N1], C2 *S, const L &lay, int j1, const C2 *__restrict__ tw) {
   constexpr int N2 = N / N1;
 #pragma unroll
   for (int c = 0; c < N2 / N1; c++) {
     const int k2 = j1 + N1 * c;
-    double2 b[N1];
+    C2 b[N1];
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) b[k1] = a[c * N1 + k1];
-    Dft<N1, INV>::run(b);
+    Dft<N1, INV, C2>::run(b);
 #pragma unroll
     for (int n1 = 0; n1 < N1; n1++) {
-      double2 t = tw[n1 * k2];
+      C2 t = tw[n1 * k2];
       if (INV) t.y = -t.y;
-      S[lay.at(k2, n1, N1)] = (n1 == 0 || k2 == 0) ? b[n1] : cmul(b[n1], t);
+      S[lay.at(k2, n1, N1)] = (n1 == 0 || k2 == 0) ? b[n1] : mul(b[n1], t);
     }
   }
   __syncthreads();
 #pragma unroll
   for (int k2 = 0; k2 < N2; k2++) a[k2] = S[lay.at(k2, j1, N1)];
-  Dft<N2, INV>::run(a);
+  Dft<N2, INV, C2>::run(a);
   __syncthreads();
 }
 

@@ -19,6 +19,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -456,6 +457,29 @@ static double bforce_ot(double eps, double sigma, double hc) {
   return pi4 * eps4 * s12 / (9.0 * pow(hc, 9)) - pi4 * eps4 * s6 / (3.0 * pow(hc, 3));
 }
 
+__global__ void k_narrow(const double *__restrict__ in, float *__restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+__global__ void k_widen(const float *__restrict__ in, double *__restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+static unsigned cast_grid(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+int narrow(Handle *h, const double *in, float *out, size_t n) {
+  k_narrow<<<cast_grid(n), 256, 0, h->stream>>>(in, out, n);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+int widen(Handle *h, const float *in, double *out, size_t n) {
+  k_widen<<<cast_grid(n), 256, 0, h->stream>>>(in, out, n);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
 int setup_kernels(Handle *h) {
   const he4_params &P = h->p;
   const int nx = h->nx, ny = h->ny, nz = h->nz;
@@ -515,6 +539,18 @@ int setup_kernels(Handle *h) {
       off += n3[ax];
     }
     HE4_CUDA_TRY(cudaMemcpyAsync(h->dsym, ds.data(), sizeof(double) * ds.size(), cudaMemcpyHostToDevice, h->stream));
+    if (h->fp32) {
+      std::vector<float> ds32(ds.size());
+      for (size_t i = 0; i < ds.size(); i++) ds32[i] = (float)ds[i];
+      HE4_CUDA_TRY(cudaMemcpyAsync(h->dsym32, ds32.data(), sizeof(float) * ds32.size(), cudaMemcpyHostToDevice,
+                                   h->stream));
+      HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+  }
+  // FP32 copies of the k-space kernels for the FP32-convolution form
+  if (h->fp32) {
+    const double *src[4] = {h->wcgk, h->fvlj4, h->kalfs, h->vq};
+    for (int i = 0; i < 4; i++) HE4_TRY(narrow(h, src[i], h->k32[i], h->H));
   }
   // timec (DFT4He3d.f90:773-782), real part rounded to single precision
   {

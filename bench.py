@@ -121,6 +121,16 @@ def dist_setup(n_gpus):
     return rank, world, local, dist
 
 
+FORMS = {"fp64": "plain FP64", "fp32": "FP32 convolutions (FP32 half spectra, kernels and twiddles; "
+                                         "FP64 real grids, psi update, reductions and trajectories)"}
+
+
+def form_params(pkg, p, form):
+    q = pkg.abi.He4Params.from_buffer_copy(p)
+    q.precision = pkg.abi.HE4_PREC_FP32CONV if form == "fp32" else pkg.abi.HE4_PREC_FP64
+    return q
+
+
 def gpu_arm(args):
     import torch
     pkg = load_pkg()
@@ -130,8 +140,6 @@ def gpu_arm(args):
     p, psi, r, v, _ = w.workload(args.config, seed=1234 + rank)
     p.device = local
     dt = w.deltat_fs(DT_FS)
-    g = pkg.He4Step(p)
-    stream = torch.cuda.ExternalStream(g.stream(), device=torch.device("cuda", local))
 
     def barrier():
         torch.cuda.synchronize(local)
@@ -139,30 +147,47 @@ def gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize(local)
 
-    # ---- device-resident throughput: K PC steps after the RK starter + W PC
-    g.set_state(psi, r, v)
-    g.run(3 + args.warmup, dt)
-    barrier()
-    n0 = g.launch_count()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        err, means = g.run(args.steps, dt)
-        e1.record(stream)
-        e1.synchronize()
-    launches = g.launch_count() - n0
-    ms = e0.elapsed_time(e1)
-    clocks = clk.summary()
-    barrier()
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    if not np.all(np.isfinite(err)) or not np.all(np.isfinite(means)):
-        raise RuntimeError("non-finite step errors in the timed region")
+    def timed_run(g, stream):
+        """K PC steps from device-resident state, CUDA events on the
+        library's stream, max over ranks."""
+        g.set_state(psi, r, v)
+        g.run(3 + args.warmup, dt)
+        barrier()
+        n0 = g.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            err, means = g.run(args.steps, dt)
+            e1.record(stream)
+            e1.synchronize()
+        launches = g.launch_count() - n0
+        ms = e0.elapsed_time(e1)
+        barrier()
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        if not np.all(np.isfinite(err)) or not np.all(np.isfinite(means)):
+            raise RuntimeError("non-finite step errors in the timed region")
+        return ms, launches, clk.summary()
+
+    # ---- every form on the same workload; the headline is args.form
+    forms = {}
     sim_ps = args.steps * DT_FS * 1e-3
+    for form in ("fp64", "fp32"):
+        if form != args.form and not args.all_forms:
+            continue
+        gf = pkg.He4Step(form_params(pkg, p, form))
+        sf = torch.cuda.ExternalStream(gf.stream(), device=torch.device("cuda", local))
+        ms_f, launches_f, clocks_f = timed_run(gf, sf)
+        forms[form] = {"form": FORMS[form], "ms_per_step": ms_f / args.steps,
+                       "value": world * sim_ps / (ms_f / 3.6e6), "gpu_launches": launches_f, "clocks": clocks_f}
+        if form == args.form:
+            g, stream = gf, sf
+            ms_max, launches, clocks = ms_f, launches_f, clocks_f
+        else:
+            gf.close()
     value = world * sim_ps / (ms_max / 3.6e6)
 
     # ---- dominant-kernel roofline, measured live with CUDA events
@@ -220,13 +245,13 @@ def gpu_arm(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if args.form == "fp64" else "f32 spectra / f64 state",
         "data": "synthetic (Fermi-profile droplet, seeded Gaussian test particles)",
         "config": {
             "workload": f"{args.config}: {cfg['n']}^3 grid h={cfg['h']} A, N={cfg['n4']} He, "
                         f"{cfg['npar']} test particles at {cfg['speed_ms']:g} m/s, Morse impurity, "
-                        f"core4=OTC npd=7 icon=8, dt=1 fs, Hamming PC steps, plain FP64 form",
-            "form": "plain FP64",
+                        f"core4=OTC npd=7 icon=8, dt=1 fs, Hamming PC steps",
+            "form": FORMS[args.form],
             "parallelism": f"replicas x{world} (no data-path collective)",
             "l2": "inputs larger than L2: every grid array is >= 134 MB",
             "timed": "K predictor-corrector steps from device-resident state (he4_run)",
@@ -237,7 +262,10 @@ def gpu_arm(args):
         "gpu_launches": launches,
         "roofline": roof,
         "clocks": clocks,
+        "forms": forms,
     }
+    if "fp64" in forms and args.form != "fp64":
+        line["speedup_vs_plain_fp64"] = forms["fp64"]["ms_per_step"] / forms[args.form]["ms_per_step"]
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -269,7 +297,8 @@ def kernel_roofline(pkg, g, stream, args):
     traffic = None
     prof = os.path.join(ROOT, "profiles", "fft_passes_c3.json")
     if args.config == "c3" and os.path.exists(prof):
-        traffic = json.load(open(prof))["traffic_bytes_per_launch"].get(kname)
+        key = kname if args.form == "fp64" else f"{kname}:{args.form}"
+        traffic = json.load(open(prof))["traffic_bytes_per_launch"].get(key)
     return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -357,6 +386,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--form", default="fp32", choices=sorted(FORMS))
+    ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the other forms on the same workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

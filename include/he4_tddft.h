@@ -49,8 +49,15 @@ enum {
   HE4_POT_NULL = 2   /* V = 0 ('null' entry of Select_Pot)                  */
 };
 
-/* Arithmetic of the convolution FFTs and the pointwise potential assembly. */
-enum { HE4_PREC_FP64 = 0 };
+/* Arithmetic of the convolution FFTs and the pointwise potential assembly.
+ * HE4_PREC_FP64: everything in FP64 (the reference's arithmetic).
+ * HE4_PREC_FP32CONV: the half spectra of the convolution FFTs, their
+ *   twiddles, the k-space kernels (wcgk, fvlj4, kalfs, Vq) and the derivative
+ *   symbol are FP32; real grids, the wavefunction update, the reductions and
+ *   the particle integration stay FP64.  Needs every axis length to be a
+ *   power of two in [16, 256]; otherwise he4_create returns
+ *   HE4_E_UNSUPPORTED. */
+enum { HE4_PREC_FP64 = 0, HE4_PREC_FP32CONV = 1 };
 
 typedef struct he4_params {
   /* grid (namelist nx,ny,nz,xmax,ymax,zmax; DFT4He3d.f90:271-354) */
