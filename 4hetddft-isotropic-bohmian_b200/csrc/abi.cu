@@ -171,7 +171,7 @@ static int create(const he4_params *pin, Handle *h) {
   for (double **f : rfields) HE4_TRY(dalloc(f, N));
   HE4_TRY(dalloc(&h->counts, N));
   HE4_TRY(dalloc(&h->box, 1));
-  for (int i = 0; i < 4; i++) HE4_TRY(dalloc(&h->spec[i], H));
+  for (int i = 0; i < 6; i++) HE4_TRY(dalloc(&h->spec[i], H));
   double **pfields[] = {&h->rimp, &h->vimp, &h->aimp, &h->rimpold[0], &h->rimpold[1], &h->rimpold[2],
                         &h->vimpold[0], &h->vimpold[1], &h->vimpold[2], &h->aimpold[0], &h->aimpold[1],
                         &h->qr, &h->qv, &h->pcr, &h->pcv};
@@ -333,7 +333,8 @@ int he4_potenimp(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
   h->field_valid = 0;
-  HE4_TRY(field_potenimp(h));
+  HE4_TRY(field_potenimp(h, true));
+  h->split_valid = 0;
   return sync_and_check(h);
 }
 
@@ -341,7 +342,8 @@ int he4_poten(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
   h->field_valid = 0;
-  HE4_TRY(field_poten(h));
+  HE4_TRY(field_poten(h, true, h->pot4));
+  h->split_valid = 1;
   return sync_and_check(h);
 }
 
@@ -356,7 +358,7 @@ int he4_forceimp(he4_handle *hh) {
 int he4_field(he4_handle *hh) {
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
-  HE4_TRY(field_all(h));
+  HE4_TRY(field_all(h, true));
   return sync_and_check(h);
 }
 
@@ -455,7 +457,8 @@ int he4_energy(he4_handle *hh, he4_energies *e) {
     set_error("null energies");
     return HE4_E_ARG;
   }
-  if (!h->field_valid) HE4_TRY(field_all(h));  // energy() follows a field evaluation
+  if (!h->field_valid) HE4_TRY(field_all(h, true));  // energy() follows a field evaluation
+  if (!h->split_valid) HE4_TRY(field_split_fields(h));  // delj4, uimp of this state
   HE4_TRY(compute_energy(h, e));
   const double *v = &e->etot;
   if (!finite_all(v, 11)) {
@@ -482,6 +485,11 @@ int he4_get_field(he4_handle *hh, int32_t which, double *out) {
     return HE4_E_ARG;
   }
   const double *src = nullptr;
+  // fields a merged (time-step) evaluation leaves unwritten
+  if (h->field_valid && !h->split_valid &&
+      (which == HE4_F_UIMP || which == HE4_F_DELJ4 || which == HE4_F_UALPHAS || which == HE4_F_PENALTY ||
+       which == HE4_F_CORR))
+    HE4_TRY(field_split_fields(h));
   switch (which) {
     case HE4_F_DEN: src = h->den; break;
     case HE4_F_POT4: src = h->pot4; break;

@@ -190,6 +190,9 @@ struct Handle {
   int field_valid = 0;
   // fx, fy, fz hold the whole grid (otherwise only the force box)
   int forces_full = 0;
+  // uimp, delj4, corr, ualphas and penalty belong to the current evaluation
+  // (a merged evaluation does not write them)
+  int split_valid = 0;
   size_t red_len = 0;
   // captured PC steps (one per distinct StepState; the states repeat)
   std::vector<StepGraph> graphs;
@@ -212,6 +215,15 @@ struct ZOp {
   int boxz = 0;   // store only the z planes of the force box (see force_range)
 };
 int fft_z_conv(Handle *h, int n, const ZOp *ops);
+// z pass of a sum of convolutions: out = IFFT_z(sum_j coef_j K_j FFT_z(in_j))
+// (register-path z lengths only; at most 4 terms)
+struct ZTerm {
+  const double2 *in;
+  const double *kern;
+  double coef;
+};
+int fft_z_sum(Handle *h, int nterm, const ZTerm *terms, double2 *out);
+bool fft_z_sum_ok(const Handle *h);
 // inverse y and x passes restricted to the pencils and rows of the force box
 int fft_c2r_box(Handle *h, int n, double2 *const *in, double *const *out);
 
@@ -241,14 +253,22 @@ int setup_kernels(Handle *h);
 int narrow(Handle *h, const double *in, float *out, size_t n);
 int widen(Handle *h, const float *in, double *out, size_t n);
 
-int field_potenimp(Handle *h);
-int field_poten(Handle *h);
+// split: also write the named intermediate fields (uimp; delj4, corr,
+// ualphas, penalty) the way the reference's routines do; otherwise (the time
+// step path) the linear convolutions entering pot4 share one inverse FFT.
+// pot4: where the split poten writes its pot4.
+int field_potenimp(Handle *h, bool split);
+int field_poten(Handle *h, bool split, double *pot4);
 // full: the force field on the whole grid; otherwise only where the gather
 // reads it (a time step's need).  field_forces recomputes just the field.
 int field_forceimp(Handle *h, bool full);
 int field_forces(Handle *h, bool full);
-// potenimp + poten + forceimp; marks the fields valid
-int field_all(Handle *h);
+// potenimp + poten + forceimp; marks the fields valid.  split = false takes
+// the merged form when the z length allows it.
+int field_all(Handle *h, bool split = false);
+// after a merged evaluation: compute the named intermediate fields of the
+// same state without touching pot4
+int field_split_fields(Handle *h);
 // impurity.cu: denx, psix, hpsix on the particle box; quantum force term;
 // reset of the box to the whole grid
 int impurity_density(Handle *h);

@@ -709,6 +709,46 @@ int fft_z_conv(Handle *h, int n, const ZOp *ops) {
   return HE4_OK;
 }
 
+template <typename C2>
+static int zsum_reg(Handle *h, int nterm, const ZTerm *terms, double2 *out) {
+  const FftPlan &P = h->fft;
+  ZSumArgs<C2> a{};
+  a.map.nxh = P.nxh;
+  a.map.nother = P.ny;
+  a.map.so = P.nxh;
+  a.sf = (long)P.ny * P.nxh;
+  a.tw = twid<C2>(P.az);
+  a.nterm = nterm;
+  for (int j = 0; j < nterm; j++) {
+    a.t[j].in = reinterpret_cast<const C2 *>(terms[j].in);
+    a.t[j].kern = kern_of<C2>(h, terms[j].kern);
+    a.t[j].coef = terms[j].coef;
+    if (!a.t[j].kern) {
+      set_error("z-pass sum term without a kernel");
+      return HE4_E_ARG;
+    }
+  }
+  a.out = reinterpret_cast<C2 *>(out);
+  const long total = (long)P.nxh * P.ny;
+  HE4_REG_SWITCH(P.nz, {
+    constexpr int W = kRegThreads / RegShape<NN>::N1;
+    a.map.W = W;
+    k_zsum_reg<NN, C2><<<(unsigned)((total + W - 1) / W), kRegThreads, smem_zsum<NN, C2>(), h->stream>>>(a);
+  });
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+bool fft_z_sum_ok(const Handle *h) { return reg_ok(h->fft.nz); }
+
+int fft_z_sum(Handle *h, int nterm, const ZTerm *terms, double2 *out) {
+  if (nterm < 1 || nterm > kMaxTerms || !fft_z_sum_ok(h)) {
+    set_error("fft_z_sum: %d terms, z length %d", nterm, h->fft.nz);
+    return HE4_E_ARG;
+  }
+  return h->fp32 ? zsum_reg<float2>(h, nterm, terms, out) : zsum_reg<double2>(h, nterm, terms, out);
+}
+
 int fft_z_only(Handle *h, double2 *buf, bool inverse) {
   ZOp op{buf, buf, nullptr, 1.0, -1, inverse ? 2 : 1};
   return fft_z_conv(h, 1, &op);

@@ -343,8 +343,99 @@ __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
   }
 }
 
+// z pass summing several convolutions into one output:
+//   out = IFFT_z( sum_j coef_j K_j(k) FFT_z(in_j) )
+// Each term's kernel values are copied to shared memory with cp.async while
+// the term's input is loaded and transformed.
+constexpr int kMaxTerms = 4;
+template <typename C2>
+struct ZTermT {
+  const C2 *in;
+  const typename regfft::Re<C2>::type *kern;
+  double coef;
+};
+template <typename C2>
+struct ZSumArgs {
+  PencilMap map;
+  long sf;
+  const C2 *tw;
+  int nterm;
+  ZTermT<C2> t[kMaxTerms];
+  C2 *out;
+};
+
+template <int N, typename C2>
+inline size_t smem_zsum() {
+  using T = typename regfft::Re<C2>::type;
+  constexpr int N1 = RegShape<N>::N1, W = kRegThreads / N1;
+  return sizeof(C2) * ((size_t)N * W + N) + sizeof(T) * (size_t)N * W + sizeof(long) * W;
+}
+
+template <int N, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_zsum_reg(ZSumArgs<C2> a) {
+  using T = typename regfft::Re<C2>::type;
+  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kRegThreads / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
+  T *Ks = reinterpret_cast<T *>(tw + N);  // [N][W]
+  long *offs = reinterpret_cast<long *>(Ks + N * W);
+  load_tw_n<N>(tw, a.tw);
+  if (threadIdx.x < W) {
+    int kx, o;
+    offs[threadIdx.x] = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
+  }
+  __syncthreads();
+  auto prefetch = [&](int j) {
+    const T *kern = a.t[j].kern;
+    for (int e = threadIdx.x; e < N * W; e += kRegThreads) {
+      const int ww = e % W, k = e / W;
+      const long of = offs[ww];
+      if (of >= 0) __pipeline_memcpy_async(Ks + e, kern + of + (long)k * a.sf, sizeof(T));
+    }
+  };
+  prefetch(0);
+  __pipeline_commit();
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  const long off = offs[w];
+  regfft::LayoutYZ lay{W, w};
+  C2 acc[N2];
+#pragma unroll
+  for (int e = 0; e < N2; e++) acc[e] = regfft::mk<C2>(0, 0);
+  for (int j = 0; j < a.nterm; j++) {
+    const C2 *in = a.t[j].in;
+    C2 v[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? in[off + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+    regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
+    __pipeline_wait_prior(0);
+    __syncthreads();  // term j's kernel values are in Ks
+    const T coef = (T)a.t[j].coef;
+#pragma unroll
+    for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) {
+        const int k = (j1 + N1 * c) + N2 * k1;
+        const T cf = (off >= 0) ? coef * Ks[k * W + w] : T(0);
+        const C2 x = v[c * N1 + k1];
+        acc[c * N1 + k1] = regfft::mk<C2>(acc[c * N1 + k1].x + cf * x.x, acc[c * N1 + k1].y + cf * x.y);
+      }
+    if (j + 1 < a.nterm) {
+      __syncthreads();  // everyone is done with Ks
+      prefetch(j + 1);
+    }
+    __pipeline_commit();
+  }
+  regfft::bwd2<N, N1, true>(acc, S, lay, j1, tw);
+  if (off >= 0) {
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) a.out[off + (j1 + N1 * n2) * a.sf] = acc[n2];
+  }
+}
+
 template <int N, typename C2>
 inline int reg_attrs() {
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zsum_reg<N, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zsum<N, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_yz_reg<N, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -96,6 +96,32 @@ __global__ void k_pot4_final(double *pot4, const double *__restrict__ uimp, cons
   if (t < n) pot4[t] = pot4[t] + uimp[t] + penalty[t];
 }
 
+// Merged assembly: lin = delj4 + uimp + sto1 + h2o2m4*alphas/den0s * u1,
+// produced by one summed inverse transform, then
+// pot4 = lin + dencg^2 (a0 + a1 dencg) + penalty + h2o2m4*alphas*sum_i d_i h_i
+// (poten.f90:80-92,101-104,122-124 and term_alfa.f90:110-113 regrouped: every
+// convolution that enters pot4 linearly shares one inverse FFT).
+template <bool OTC>
+__global__ void k_pot4_merged(const double *__restrict__ lin, const double *__restrict__ den,
+                              const double *__restrict__ dencg, const double *__restrict__ h0,
+                              const double *__restrict__ h1, const double *__restrict__ h2, double *pot4, Stencil st,
+                              Geo g, OtArgs a) {
+  HE4_IJK(g);
+  const double d = den[t];
+  const double th = tanh(a.beta * (d - a.den_m));
+  const double pen = a.c_solid * (1.0 + th + a.beta * d * (1.0 - th * th));
+  const double dc = dencg[t];
+  const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0;
+  double v = lin[t] + dc * dc * (a0 + a1 * dc) + pen;
+  if (OTC) {
+    const double d0 = stencil_axis(h0, st.w1[0], st.m, g, i, j, k, 0);
+    const double d1 = stencil_axis(h1, st.w1[1], st.m, g, i, j, k, 1);
+    const double d2 = stencil_axis(h2, st.w1[2], st.m, g, i, j, k, 2);
+    v += (d0 + d1 + d2) * a.h2o2m4 * a.alphas;
+  }
+  pot4[t] = v;
+}
+
 // ---------------------------------------------------------------------------
 // gather of the force field at the particles
 // ---------------------------------------------------------------------------
@@ -153,21 +179,97 @@ static OtArgs ot_args(const Handle *h) {
 
 static inline unsigned nblk(size_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
-int field_potenimp(Handle *h) {
+int field_potenimp(Handle *h, bool split) {
   // denpart: denx, psix, hpsix on the particle box (impurity.cu)
   HE4_TRY(impurity_density(h));
-  // uimp = IFFT(FFT(denx) * Vq) * renor (potenimp.f90:17-19)
+  // x/y transform of denx, kept in spec[4] for the merged assembly
   const double *in[1] = {h->denx};
-  double2 *sp[1] = {h->spec[1]};
+  double2 *sp[1] = {h->spec[4]};
   HE4_TRY(fft_r2c(h, 1, in, sp));
-  ZOp op{h->spec[1], h->spec[1], h->vq, h->renor, -1};
+  if (!split) return HE4_OK;
+  // uimp = IFFT(FFT(denx) * Vq) * renor (potenimp.f90:17-19)
+  ZOp op{h->spec[4], h->spec[1], h->vq, h->renor, -1};
   HE4_TRY(fft_z_conv(h, 1, &op));
+  double2 *so[1] = {h->spec[1]};
   double *out[1] = {h->uimp};
-  HE4_TRY(fft_c2r(h, 1, sp, out));
+  HE4_TRY(fft_c2r(h, 1, so, out));
   return HE4_OK;
 }
 
-int field_poten(Handle *h) {
+// Merged form of poten (the time-step path): the linear convolutions that
+// enter pot4 (delj4, uimp, the correlation term and the alpha_s u1 term) are
+// summed in k space and inverted once; the named intermediate fields delj4,
+// uimp, corr, ualphas and penalty are not written.
+static int field_poten_merged(Handle *h) {
+  const Geo g = geo(h);
+  const size_t N = h->N;
+  const OtArgs ot = ot_args(h);
+  const bool otc = (h->p.core4 == HE4_CORE_OTC);
+  {
+    const double *in[1] = {h->den};
+    double2 *sp[1] = {h->spec[0]};
+    HE4_TRY(fft_r2c(h, 1, in, sp));
+  }
+  // dencg and denalf (poten.f90:34-38, 95-99)
+  {
+    ZOp ops[2] = {{h->spec[0], h->spec[1], h->wcgk, h->renor, -1}, {h->spec[0], h->spec[3], h->kalfs, h->renor, -1}};
+    HE4_TRY(fft_z_conv(h, otc ? 2 : 1, ops));
+    double2 *sp[2] = {h->spec[1], h->spec[3]};
+    double *out[2] = {h->dencg, h->denalf};
+    HE4_TRY(fft_c2r(h, otc ? 2 : 1, sp, out));
+  }
+  k_grad<<<grid3(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+  HE4_LAUNCHED(h);
+  // correlation source, x/y transform kept in spec[5]
+  k_corr_src<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->rtmp[0], N, ot);
+  HE4_LAUNCHED(h);
+  {
+    const double *in[1] = {h->rtmp[0]};
+    double2 *sp[1] = {h->spec[5]};
+    HE4_TRY(fft_r2c(h, 1, in, sp));
+  }
+  ZTerm terms[4] = {{h->spec[0], h->fvlj4, h->renor}, {h->spec[4], h->vq, h->renor}, {h->spec[5], h->wcgk, h->renor},
+                    {h->spec[1], h->kalfs, h->renor * h->p.h2o2m4 * h->p.alphas / h->p.den0s}};
+  if (otc) {
+    k_alfa1<<<nblk(N), 256, 0, h->stream>>>(h->denalf, h->dxden, h->dyden, h->dzden, h->falfs, h->rtmp[0],
+                                           h->rtmp[1], h->rtmp[2], N, ot);
+    HE4_LAUNCHED(h);
+    {
+      const double *in[3] = {h->rtmp[0], h->rtmp[1], h->rtmp[2]};
+      double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
+      HE4_TRY(fft_r2c(h, 3, in, sp));
+      ZOp ops[3] = {{h->spec[1], h->spec[1], h->kalfs, h->renor, -1},
+                    {h->spec[2], h->spec[2], h->kalfs, h->renor, -1},
+                    {h->spec[3], h->spec[3], h->kalfs, h->renor, -1}};
+      HE4_TRY(fft_z_conv(h, 3, ops));
+      double *out[3] = {h->intx, h->inty, h->intz};
+      HE4_TRY(fft_c2r(h, 3, sp, out));
+    }
+    k_alfa2<<<nblk(N), 256, 0, h->stream>>>(h->dxden, h->dyden, h->dzden, h->intx, h->inty, h->intz, h->falfs,
+                                           h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], N);
+    HE4_LAUNCHED(h);
+    const double *in[1] = {h->rtmp[0]};
+    double2 *sp[1] = {h->spec[1]};
+    HE4_TRY(fft_r2c(h, 1, in, sp));
+  }
+  HE4_TRY(fft_z_sum(h, otc ? 4 : 3, terms, h->spec[2]));
+  {
+    double2 *sp[1] = {h->spec[2]};
+    double *out[1] = {h->rtmp[0]};
+    HE4_TRY(fft_c2r(h, 1, sp, out));
+  }
+  if (otc)
+    k_pot4_merged<true><<<grid3(g), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h->rtmp[1], h->rtmp[2],
+                                                              h->rtmp[3], h->pot4, h->st, g, ot);
+  else
+    k_pot4_merged<false><<<grid3(g), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, nullptr, nullptr,
+                                                               nullptr, h->pot4, h->st, g, ot);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+int field_poten(Handle *h, bool split, double *pot4) {
+  if (!split) return field_poten_merged(h);
   const Geo g = geo(h);
   const size_t N = h->N;
   const OtArgs ot = ot_args(h);
@@ -204,7 +306,7 @@ int field_poten(Handle *h) {
     double *out[1] = {h->corr};
     HE4_TRY(fft_c2r(h, 1, sp, out));
   }
-  k_pot4_base<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->delj4, h->corr, h->penalty, h->pot4, N, ot);
+  k_pot4_base<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->delj4, h->corr, h->penalty, pot4, N, ot);
   HE4_LAUNCHED(h);
   // term_alfa (term_alfa.f90:28-113), called for core4='OTC' only
   // (poten.f90:94-105).
@@ -235,11 +337,11 @@ int field_poten(Handle *h) {
       double *out[1] = {h->ualphas};
       HE4_TRY(fft_c2r(h, 1, sp, out));
     }
-    k_alfa3<<<grid3(g), block3(), 0, h->stream>>>(h->ualphas, h->rtmp[1], h->rtmp[2], h->rtmp[3], h->pot4, h->st,
+    k_alfa3<<<grid3(g), block3(), 0, h->stream>>>(h->ualphas, h->rtmp[1], h->rtmp[2], h->rtmp[3], pot4, h->st,
                                                   g, ot);
     HE4_LAUNCHED(h);
   }
-  k_pot4_final<<<nblk(N), 256, 0, h->stream>>>(h->pot4, h->uimp, h->penalty, N);
+  k_pot4_final<<<nblk(N), 256, 0, h->stream>>>(pot4, h->uimp, h->penalty, N);
   HE4_LAUNCHED(h);
   return HE4_OK;
 }

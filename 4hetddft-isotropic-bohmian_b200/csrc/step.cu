@@ -253,12 +253,24 @@ int compute_den(Handle *h) {
   return HE4_OK;
 }
 
-int field_all(Handle *h) {
+int field_all(Handle *h, bool split) {
+  split = split || !fft_z_sum_ok(h);
   h->field_valid = 0;
-  HE4_TRY(field_potenimp(h));
-  HE4_TRY(field_poten(h));
+  h->split_valid = 0;
+  HE4_TRY(field_potenimp(h, split));
+  HE4_TRY(field_poten(h, split, h->pot4));
   HE4_TRY(field_forceimp(h, false));
   h->field_valid = 1;
+  h->split_valid = split ? 1 : 0;
+  return HE4_OK;
+}
+
+int field_split_fields(Handle *h) {
+  // the split poten writes its pot4 into spec[5], free outside an evaluation
+  // (2 (nx/2+1) >= nx reals per row)
+  HE4_TRY(field_potenimp(h, true));
+  HE4_TRY(field_poten(h, true, reinterpret_cast<double *>(h->spec[5])));
+  h->split_valid = 1;
   return HE4_OK;
 }
 
