@@ -24,6 +24,12 @@ HE4_POT_NULL = 2
 HE4_PREC_FP64 = 0
 HE4_PREC_FP32CONV = 1
 
+HE4_D_PSI = 0
+HE4_D_RIMP = 1
+HE4_D_VIMP = 2
+HE4_D_DEN = 3
+HE4_D_DENX = 4
+
 FIELDS = [
     "den", "pot4", "denx", "psix", "hpsix", "uimp", "dencg", "delj4", "denalf",
     "ualphas", "falfs", "intxalf", "intyalf", "intzalf", "dxden", "dyden",

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhe4b200.so")
-SOURCES = ["abi.cu", "fft.cu", "setup.cu", "field.cu", "impurity.cu", "step.cu", "energy.cu", "diag.cu"]
+SOURCES = ["abi.cu", "fft.cu", "setup.cu", "field.cu", "impurity.cu", "step.cu", "energy.cu", "diag.cu", "fno.cu"]
 HEADERS = ["common.cuh", "stencil.cuh", "reduce.cuh", "fft_reg.cuh", "fft_passes.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -27,6 +27,7 @@ def _stale():
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(HERE, "..", "include", "he4_tddft.h"))
+    deps.append(os.path.join(HERE, "..", "include", "he4_fno.h"))
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps)
 

@@ -293,9 +293,9 @@ int he4_set_state(he4_handle *hh, const double *psi, const double *rimp, const d
     return HE4_E_ARG;
   }
   const size_t N = h->N, P3 = 3 * (size_t)h->npar;
-  HE4_CUDA_TRY(cudaMemcpyAsync(h->psi, psi, sizeof(double2) * N, cudaMemcpyHostToDevice, h->stream));
-  HE4_CUDA_TRY(cudaMemcpyAsync(h->rimp, rimp, sizeof(double) * P3, cudaMemcpyHostToDevice, h->stream));
-  HE4_CUDA_TRY(cudaMemcpyAsync(h->vimp, vimp, sizeof(double) * P3, cudaMemcpyHostToDevice, h->stream));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->psi, psi, sizeof(double2) * N, cudaMemcpyDefault, h->stream));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->rimp, rimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->vimp, vimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
   HE4_CUDA_TRY(cudaMemsetAsync(h->aimp, 0, sizeof(double) * P3, h->stream));
   double2 *cz[] = {h->psiold[0], h->psiold[1], h->psiold[2], h->hpsiold[0], h->hpsiold[1], h->pc, h->q};
   for (double2 *f : cz) HE4_CUDA_TRY(cudaMemsetAsync(f, 0, sizeof(double2) * N, h->stream));
@@ -316,10 +316,10 @@ int he4_get_state(he4_handle *hh, double *psi, double *rimp, double *vimp, doubl
   HANDLE_OR_FAIL(hh);
   NEED_STATE(h);
   const size_t P3 = 3 * (size_t)h->npar;
-  if (psi) HE4_CUDA_TRY(cudaMemcpyAsync(psi, h->psi, sizeof(double2) * h->N, cudaMemcpyDeviceToHost, h->stream));
-  if (rimp) HE4_CUDA_TRY(cudaMemcpyAsync(rimp, h->rimp, sizeof(double) * P3, cudaMemcpyDeviceToHost, h->stream));
-  if (vimp) HE4_CUDA_TRY(cudaMemcpyAsync(vimp, h->vimp, sizeof(double) * P3, cudaMemcpyDeviceToHost, h->stream));
-  if (aimp) HE4_CUDA_TRY(cudaMemcpyAsync(aimp, h->aimp, sizeof(double) * P3, cudaMemcpyDeviceToHost, h->stream));
+  if (psi) HE4_CUDA_TRY(cudaMemcpyAsync(psi, h->psi, sizeof(double2) * h->N, cudaMemcpyDefault, h->stream));
+  if (rimp) HE4_CUDA_TRY(cudaMemcpyAsync(rimp, h->rimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
+  if (vimp) HE4_CUDA_TRY(cudaMemcpyAsync(vimp, h->vimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
+  if (aimp) HE4_CUDA_TRY(cudaMemcpyAsync(aimp, h->aimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return HE4_OK;
 }
@@ -656,6 +656,25 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
   if (name && name_len > 0) {
     strncpy(name, names[which], name_len - 1);
     name[name_len - 1] = 0;
+  }
+  return HE4_OK;
+}
+
+int he4_device_ptr(he4_handle *hh, int32_t which, void **ptr) {
+  HANDLE_OR_FAIL(hh);
+  if (!ptr) {
+    set_error("null output");
+    return HE4_E_ARG;
+  }
+  switch (which) {
+    case HE4_D_PSI: *ptr = h->psi; break;
+    case HE4_D_RIMP: *ptr = h->rimp; break;
+    case HE4_D_VIMP: *ptr = h->vimp; break;
+    case HE4_D_DEN: *ptr = h->den; break;
+    case HE4_D_DENX: *ptr = h->denx; break;
+    default:
+      set_error("unknown device array id %d", which);
+      return HE4_E_ARG;
   }
   return HE4_OK;
 }

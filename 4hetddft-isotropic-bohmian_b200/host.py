@@ -53,6 +53,7 @@ def load_library():
     L.he4_diagnostics.argtypes = [vp, i32, dp]
     L.he4_get_kernel.argtypes = [vp, i32, dp]
     L.he4_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.he4_device_ptr.argtypes = [vp, i32, C.POINTER(vp)]
     L.he4_launch_count.argtypes = [vp]
     L.he4_launch_count.restype = C.c_int64
     L.he4_strerror.argtypes = [C.c_int]
@@ -108,6 +109,27 @@ class He4Step:
 
     def __exit__(self, *exc):
         self.close()
+
+    def device_ptr(self, which):
+        """Device address of a state array: 'psi', 'rimp', 'vimp', 'den',
+        'denx' (he4_device_ptr)."""
+        ids = {"psi": abi.HE4_D_PSI, "rimp": abi.HE4_D_RIMP, "vimp": abi.HE4_D_VIMP, "den": abi.HE4_D_DEN,
+               "denx": abi.HE4_D_DENX}
+        out = C.c_void_p()
+        _check(load_library().he4_device_ptr(self._h, ids[which], C.byref(out)), "he4_device_ptr")
+        return out.value
+
+    def set_state_device(self, psi_ptr, rimp_ptr, vimp_ptr):
+        """he4_set_state from device arrays (addresses as integers)."""
+        dpp = lambda a: C.cast(C.c_void_p(a), C.POINTER(C.c_double))
+        _check(load_library().he4_set_state(self._h, dpp(psi_ptr), dpp(rimp_ptr), dpp(vimp_ptr)),
+               "he4_set_state")
+
+    def get_state_device(self, psi_ptr, rimp_ptr, vimp_ptr):
+        """he4_get_state into device arrays (addresses as integers, 0 = skip)."""
+        dpp = lambda a: C.cast(C.c_void_p(a), C.POINTER(C.c_double)) if a else None
+        _check(load_library().he4_get_state(self._h, dpp(psi_ptr), dpp(rimp_ptr), dpp(vimp_ptr), None),
+               "he4_get_state")
 
     # readenc mode 2 / printoutc
     def set_state(self, psi, rimp, vimp):

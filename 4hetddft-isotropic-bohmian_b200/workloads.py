@@ -111,3 +111,21 @@ def workload(name, seed=1234, **overrides):
     psi = droplet_psi(p, cfg["n4"])
     rimp, vimp = particles(cfg["npar"], seed, cfg["speed_ms"])
     return p, psi, rimp, vimp, cfg["steps"]
+
+
+def family_member(name, seed):
+    """One seeded member of a configuration's family (the training
+    trajectories of the FNO coarse propagator): the same droplet and grid,
+    the impurity cloud started at a random point 1.5-3 A off centre (random
+    direction) with a speed drawn uniformly from [50, 200] m/s toward the
+    centre.  Returns (params, psi, rimp, vimp)."""
+    cfg = CONFIGS[name]
+    rng = np.random.Generator(np.random.PCG64(seed))
+    d = rng.standard_normal(3)
+    d /= np.linalg.norm(d)
+    center = d * rng.uniform(1.5, 3.0)
+    speed = rng.uniform(50.0, 200.0)
+    p = make_params(cfg["n"], cfg["h"], cfg["npar"])
+    psi = droplet_psi(p, cfg["n4"])
+    rimp, vimp = particles(cfg["npar"], seed, speed, center=tuple(center))
+    return p, psi, rimp, vimp

@@ -118,7 +118,10 @@ void he4_destroy(he4_handle *h);
 /* readenc mode 2 (readenc.f90:96-114): psi [nz][ny][nx] complex, rimp and
  * vimp [3][n_par].  Also sets den=|psi|^2 (readenc.f90:102), zeroes the
  * RK/PC histories (dimen.f90:75-79,133-134; DFT4He3d.f90:841-845) and makes
- * the next he4_run/he4_step call start with the RK-Gill starter. */
+ * the next he4_run/he4_step call start with the RK-Gill starter.
+ * The arrays of he4_set_state and he4_get_state may be host or device
+ * memory (unified addressing); device arrays written on another stream must
+ * be complete before the call. */
 int he4_set_state(he4_handle *h, const double *psi, const double *rimp,
                   const double *vimp);
 /* printoutc inputs (printoutc.f90:139-142) plus aimp. Any pointer may be NULL. */
@@ -197,6 +200,12 @@ int he4_bench_kernel(he4_handle *h, int32_t which, int32_t reps, double *ms_per_
 
 /* Stream the handle launches on (cudaStream_t), for event timing. */
 int he4_get_stream(he4_handle *h, void **stream);
+/* Device address of one of the handle's state arrays, for device-side
+ * coupling (the parareal driver, the FNO data pipeline): psi complex
+ * [nz][ny][nx], rimp / vimp [3][n_par], den and denx [nz][ny][nx].  Valid
+ * until he4_destroy; work on them must be ordered with the handle's stream. */
+enum { HE4_D_PSI = 0, HE4_D_RIMP = 1, HE4_D_VIMP = 2, HE4_D_DEN = 3, HE4_D_DENX = 4 };
+int he4_device_ptr(he4_handle *h, int32_t which, void **ptr);
 /* Number of kernels this handle has launched (graph launches count the
  * kernels inside the graph). */
 int64_t he4_launch_count(he4_handle *h);

@@ -27,7 +27,7 @@ def lib(pkg):
 
 
 def declared_functions():
-    src = open(HEADER).read()
+    src = open(HEADER).read() + open(os.path.join(ROOT, "include", "he4_fno.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(he4_[a-z0-9_]+)\s*\(", src)))
 
