@@ -147,6 +147,7 @@ class Fno:
             self.mat[k + "H"] = self._cmat(a.conj().T)
         self.acts = None
         self.batch = 0
+        self.launches = 1  # kernels launched by this object (the BF16 copy above)
 
     # -- storage helpers ----------------------------------------------------
     def _cmat(self, a):
@@ -165,6 +166,8 @@ class Fno:
         for name, (off, shape, size) in self.offsets.items():
             host[off:off + size] = np.asarray(params[name], dtype=np.float32).reshape(-1)
         self.master.copy_(self.torch.from_numpy(host).to(self.dev))
+        if hasattr(self, "launches"):
+            self.launches += 1
         _check(self.L.he4_fno_to_bf16(self._p(self.master), self._p(self.bf16), self.nparam, self.sp),
                "he4_fno_to_bf16")
 
@@ -207,6 +210,7 @@ class Fno:
         self.batch = batch
 
     def _contract(self, x, y, mat, outer, J, K, inner, in_real=0, out_real=0, acc=0):
+        self.launches += 1
         _check(self.L.he4_fno_contract(self._p(x), self._p(y), self._p(self.mat[mat]), outer, J, K, inner, in_real,
                                        out_real, acc, self.sp), "he4_fno_contract")
 
@@ -219,6 +223,7 @@ class Fno:
         self._contract(a["s1"], a["s2"], "Fy", B * Cw * n, n, s.my, s.mx)
         self._contract(a["s2"], V, "Fz", B * Cw, n, s.mz, s.my * s.mx)
         _check(self.L.he4_fno_mix(self._p(V), R, self._p(a["s3"]), B, Cw, Cw, s.M, self.sp), "he4_fno_mix")
+        self.launches += 1
         self._contract(a["s3"], a["s2"], "Gz", B * Cw, s.mz, n, s.my * s.mx)
         self._contract(a["s2"], a["s1"], "Gy", B * Cw * n, s.my, n, s.mx)
         self._contract(a["s1"], out, "Gx", B * Cw * n * n, s.mx, n, 1, out_real=1)
@@ -230,6 +235,7 @@ class Fno:
         s, a, L, B = self.spec, self.acts, self.L, batch
         self._x = x
         bf, ms = self.bf16, self.master
+        self.launches += 3 + s.layers  # lift, layers, Q1, Q2 pointwise kernels
         _check(L.he4_fno_pointwise(self._p(x), self._at(bf, "P_W"), self._at(ms, "P_b"), None, None,
                                    self._p(a["h"][0]), B, s.cin, s.width, s.P, 0, self.sp), "lift")
         for l in range(s.layers):
@@ -250,6 +256,9 @@ class Fno:
         s, a, L, B = self.spec, self.acts, self.L, self.batch
         bf, g, n, Cw = self.bf16, self.grad, s.n, s.width
         w = self._p(a["work"])
+        # pointwise backward: act' (hidden layers and Q1), W^T g, weight-grad
+        # partials and their sum; mixing backward: 2 kernels per layer
+        self.launches += (3 + 4) + (s.layers - 1) * 4 + 3 + 2 * s.layers + 2
         _check(L.he4_fno_pointwise_bwd(self._p(gy), None, self._p(a["q"]), self._at(bf, "Q2_W"), self._p(a["g1"]),
                                        self._at(g, "Q2_W"), self._at(g, "Q2_b"), w, B, Cw, s.cout, s.P, 0, self.sp),
                "Q2 bwd")
@@ -284,6 +293,7 @@ class Fno:
         """Relative squared error sum (pred-target)^2 / sum target^2 on the
         device (a float64 tensor of 2: loss, sum target^2)."""
         a = self.acts
+        self.launches += 3 if grad is not None else 2
         _check(self.L.he4_fno_loss(self._p(pred), self._p(target), self._p(grad) if grad is not None else None,
                                    self._p(a["loss"]), pred.numel(), self._p(a["loss_work"]), self.sp), "loss")
         return a["loss"]
@@ -294,6 +304,7 @@ class Fno:
         loss = self.loss(y, target, a["gy"])
         self.backward(a["gy"])
         self.step_count += 1
+        self.launches += 1
         _check(self.L.he4_fno_adam(self._p(self.master), self._p(self.grad), self._p(self.m), self._p(self.v),
                                    self._p(self.bf16), self.nparam, lr, beta1, beta2, eps, self.step_count, self.sp),
                "adam")

@@ -81,6 +81,7 @@ class FnoCoarse:
         x = self.x if out is None else out
         sp = self.net.sp
         nc3 = self.nc ** 3
+        self.net.launches += 3  # restrict, deposit, deposit scaling
         _check(self.L.he4_fno_restrict(C.c_void_p(psi_ptr), C.c_void_p(x.data_ptr()), self.nf, self.f, 1,
                                        PSI_SCALE, sp), "he4_fno_restrict")
         _check(self.L.he4_fno_deposit(C.c_void_p(r_ptr), npar, C.c_void_p(x.data_ptr() + 8 * nc3), self.nc,
@@ -94,6 +95,7 @@ class FnoCoarse:
         x = self.encode(src.psi.data_ptr(), src.r.data_ptr(), npar)
         y = self.net.predict(x, 1)
         dst.psi.copy_(src.psi)
+        self.net.launches += 1
         _check(self.L.he4_fno_prolong_add(C.c_void_p(y.data_ptr()), C.c_void_p(dst.psi.data_ptr()), self.nf,
                                           self.f, 1.0 / (PSI_SCALE * OUT_GAIN), self.net.sp), "he4_fno_prolong_add")
         dst.r.copy_(src.r).add_(src.v, alpha=self.dt)
@@ -272,14 +274,19 @@ class Parareal:
             self.fine_steps += self.steps
         torch.cuda.synchronize(self.dev)
 
-    def run(self, psi0, r0, v0, tol=1e-6, max_iter=None, fallback=True, contraction=0.5, log=None):
+    def run(self, psi0, r0, v0, tol=1e-6, max_iter=None, fallback=True, contraction=0.5, first_change_max=0.1,
+            log=None):
         """Returns a dict: iterations, per-iteration max relative psi change,
         wall seconds (device-synchronised), fine steps executed, and where the
         sequential fallback took over.  fallback: when an iteration does not
         shrink the change by `contraction`, or a fine run leaves the range
         the solver integrates, the remaining slices are integrated one after
         the other from the last exact boundary (the plain integrator is both
-        the fallback and the judge of the coarse propagator)."""
+        the fallback and the judge of the coarse propagator).  The first
+        iteration's change is the coarse propagator's error over one slice as
+        the fine propagator judges it; above first_change_max the remaining
+        iterations cannot reach `tol` in fewer fine sweeps than the slices
+        left, so the fallback starts right away."""
         torch = self.torch
         max_iter = self.S if max_iter is None else max_iter
         t0 = time.perf_counter()
@@ -289,6 +296,9 @@ class Parareal:
         self.U[0].v.copy_(torch.from_numpy(np.ascontiguousarray(v0)))
         torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
         # initial coarse sweep
         for n in range(self.S):
             self.G(self.U[n], self.U[n + 1])
@@ -327,14 +337,21 @@ class Parareal:
             if change <= tol:
                 converged = True
                 break
-            if fallback and k >= 2 and change > contraction * history[-2]:
+            if fallback and k < self.S and ((k == 1 and change > first_change_max) or
+                                            (k >= 2 and change > contraction * history[-2])):
                 fallback_at = k
                 self._sequential(k)
                 break
+        # every stream is idle here, so the interval between the two events
+        # on the current stream spans all device work of the run
         torch.cuda.synchronize(self.dev)
+        ev1.record()
+        ev1.synchronize()
         wall = time.perf_counter() - t0
+        device_s = ev0.elapsed_time(ev1) * 1e-3
         return {"iterations": k, "converged": converged or fallback_at is not None, "diverged": diverged,
-                "fallback_at": fallback_at, "changes": history, "wall_s": wall, "fine_steps": self.fine_steps}
+                "fallback_at": fallback_at, "changes": history, "wall_s": wall, "device_s": device_s,
+                "fine_steps": self.fine_steps}
 
     def final_state(self):
         return self.U[self.S]

@@ -106,23 +106,47 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """One process per GPU (torchrun env); the replicas share nothing but
+    the timing reduction.  backend "gloo" runs the same plumbing on CPU."""
     if n_gpus <= 1 and "RANK" not in os.environ:
         return 0, 1, 0, None
+    import datetime
+
     import torch
     import torch.distributed as dist
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    import datetime
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                            device_id=torch.device("cuda", local))
+    kw = {}
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        kw["device_id"] = torch.device("cuda", local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600), **kw)
     return rank, world, local, dist
 
 
+def max_over_ranks(dist, x, device):
+    """The largest value of x over all ranks (x itself without a group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, sim_ps_per_rank, seconds_max):
+    """Whole-job simulated ps per hour: every rank advanced its own replica
+    by sim_ps_per_rank in at most seconds_max (the slowest rank)."""
+    return world * sim_ps_per_rank / (seconds_max / 3600.0)
+
+
 FORMS = {"fp64": "plain FP64", "fp32": "FP32 convolutions (FP32 half spectra, kernels and twiddles; "
-                                         "FP64 real grids, psi update, reductions and trajectories)"}
+                                         "FP64 real grids, psi update, reductions and trajectories)",
+         "parareal": "learned parareal: FNO coarse step (64^3, width 32, 12 modes/axis, 4 layers, BF16 weights) "
+                     "+ FP32-convolution PC fine propagator over 16 slices of 50 fs, sequential fallback"}
+PARAREAL_SLICES, PARAREAL_STEPS = 16, 50
 
 
 def form_params(pkg, p, form):
@@ -164,10 +188,7 @@ def gpu_arm(args):
         launches = g.launch_count() - n0
         ms = e0.elapsed_time(e1)
         barrier()
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(dist, ms, f"cuda:{local}")
         if not np.all(np.isfinite(err)) or not np.all(np.isfinite(means)):
             raise RuntimeError("non-finite step errors in the timed region")
         return ms, launches, clk.summary()
@@ -175,23 +196,38 @@ def gpu_arm(args):
     # ---- every form on the same workload; the headline is args.form
     forms = {}
     sim_ps = args.steps * DT_FS * 1e-3
+    step_form = "fp32" if args.form == "parareal" else args.form
     for form in ("fp64", "fp32"):
-        if form != args.form and not args.all_forms:
+        if form != step_form and not args.all_forms:
             continue
         gf = pkg.He4Step(form_params(pkg, p, form))
         sf = torch.cuda.ExternalStream(gf.stream(), device=torch.device("cuda", local))
         ms_f, launches_f, clocks_f = timed_run(gf, sf)
         forms[form] = {"form": FORMS[form], "ms_per_step": ms_f / args.steps,
-                       "value": world * sim_ps / (ms_f / 3.6e6), "gpu_launches": launches_f, "clocks": clocks_f}
-        if form == args.form:
+                       "value": replica_throughput(world, sim_ps, ms_f * 1e-3), "gpu_launches": launches_f,
+                       "clocks": clocks_f}
+        if form == step_form:
             g, stream = gf, sf
             ms_max, launches, clocks = ms_f, launches_f, clocks_f
         else:
             gf.close()
-    value = world * sim_ps / (ms_max / 3.6e6)
+    value = replica_throughput(world, sim_ps, ms_max * 1e-3)
 
     # ---- dominant-kernel roofline, measured live with CUDA events
-    roof = kernel_roofline(pkg, g, stream, args)
+    roof = kernel_roofline(pkg, g, stream, args, step_form)
+
+    par = None
+    if args.form == "parareal":
+        par = parareal_form(pkg, args, p, psi, r, v, dt, local, barrier)
+        dev_s = max_over_ranks(dist, par["device_s"], f"cuda:{local}")
+        par["e2e_s"] = max_over_ranks(dist, par["e2e_s"], f"cuda:{local}")
+        par["value"] = replica_throughput(world, par["sim_ps"], dev_s)
+        par["ms_per_step"] = dev_s * 1e3 / (PARAREAL_SLICES * PARAREAL_STEPS)
+        forms["parareal"] = par
+        value = par["value"]
+        ms_max = par["ms_per_step"]
+        launches = par["gpu_launches"]
+        clocks = par["clocks"]
 
     # ---- end to end through the per-step C ABI with host buffers:
     # he4_set_state (pinned host -> device), 3 he4_step_rk + (K-3)
@@ -216,14 +252,20 @@ def gpu_arm(args):
             raise RuntimeError(f"step failed: {rc}")
     assert L.he4_get_state(g._h, dp(out_psi), dp(out_r), None, None) == 0
     t1 = time.perf_counter()
-    e2e_s = t1 - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(dist, t1 - t0, f"cuda:{local}")
     h2d = psi.nbytes + r.nbytes + v.nbytes
     d2h = psi.nbytes + r.nbytes + (3 * 8 + 9 * 8) * (e2e_steps - 3) + 9 * 8 * 3
-    e2e_value = world * e2e_steps * DT_FS * 1e-3 / (e2e_s / 3600.0)
+    e2e_value = replica_throughput(world, e2e_steps * DT_FS * 1e-3, e2e_s)
+
+    if par is not None:
+        # end to end = the parareal run from host buffers to the final state
+        # on the host (initial upload, training excluded, final download)
+        e2e_value = replica_throughput(world, par["sim_ps"], par["e2e_s"])
+        h2d, d2h = par["e2e_h2d"], par["e2e_d2h"]
+        e2e_steps = PARAREAL_SLICES * PARAREAL_STEPS
+        e2e_note = "parareal run from host state: upload, iterations, fallback, final-state download"
+    else:
+        e2e_note = "3 RK-Gill starter steps, per-step err/means copy-out, state upload and download"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -239,13 +281,14 @@ def gpu_arm(args):
         "value": value,
         "unit": "simulated ps/hour",
         "n_gpus": world,
-        "steps": args.steps,
+        "steps": args.steps if par is None else PARAREAL_SLICES * PARAREAL_STEPS,
         "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps,
+        "ms_per_step": ms_max / args.steps if par is None else ms_max,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if args.form == "fp64" else "f32 spectra / f64 state",
+        "dtype": {"fp64": "f64", "fp32": "f32 spectra / f64 state",
+                  "parareal": "bf16 weights / f32 FNO / f32 spectra / f64 state"}[args.form],
         "data": "synthetic (Fermi-profile droplet, seeded Gaussian test particles)",
         "config": {
             "workload": f"{args.config}: {cfg['n']}^3 grid h={cfg['h']} A, N={cfg['n4']} He, "
@@ -254,11 +297,12 @@ def gpu_arm(args):
             "form": FORMS[args.form],
             "parallelism": f"replicas x{world} (no data-path collective)",
             "l2": "inputs larger than L2: every grid array is >= 134 MB",
-            "timed": "K predictor-corrector steps from device-resident state (he4_run)",
+            "timed": ("K predictor-corrector steps from device-resident state (he4_run)" if par is None else
+                      f"{PARAREAL_SLICES} x {PARAREAL_STEPS} fs of parareal from device-resident state "
+                      "(FNO training untimed)"),
         },
         "e2e": {"value": e2e_value, "unit": "simulated ps/hour", "h2d_bytes_per_step": h2d / e2e_steps,
-                "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
-                "includes": "3 RK-Gill starter steps, per-step err/means copy-out, state upload and download"},
+                "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps, "includes": e2e_note},
         "gpu_launches": launches,
         "roofline": roof,
         "clocks": clocks,
@@ -271,12 +315,79 @@ def gpu_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
+    """Train the FNO coarse propagator on solver trajectories of the 128^3
+    family (FP32 form, restricted to 64^3), then run parareal on the
+    workload: 16 slices of 50 fine steps, FP32-convolution fine propagator.
+    The timed region is the parareal run; its final state is compared with
+    the plain FP64 sequential run over the same 800 fs."""
+    import torch
+    w, pr, fno = pkg.workloads, pkg.parareal, pkg.fno
+    dev = torch.device("cuda", local)
+    S, K = PARAREAL_SLICES, PARAREAL_STEPS
+    spec = fno.FnoSpec(n=64, width=32, modes=(12, 12, 12), layers=4)
+    net = fno.Fno(spec, seed=5, device=local)
+    t_train = time.perf_counter()
+    xs, ys = [], []
+    for i in range(args.fno_traj):
+        pm, ps, rm, vm = w.family_member("c2", 10000 + i)
+        pm.device = local
+        enc = pr.FnoCoarse(net, pm, 2, K * dt)
+        a, b = pr.trajectory_pairs(w, pm, ps, rm, vm, 4, K, dt, enc, dev, form_params=form_params(pkg, pm, "fp32"))
+        xs += a
+        ys += b
+    hold_x, hold_y = xs[-4:], ys[-4:]
+    xs, ys = xs[:-4], ys[:-4]
+    before = pr.evaluate(net, hold_x, hold_y)
+    pr.train(net, xs, ys, args.fno_steps, batch=2, lr=1e-3)
+    after = pr.evaluate(net, hold_x, hold_y)
+    t_train = time.perf_counter() - t_train
+    q = form_params(pkg, p, "fp32")
+    coarse = pr.FnoCoarse(net, q, p.nx // spec.n, K * dt)
+    par = pr.Parareal(q, S, K, dt, coarse, concurrent=8)
+    n_lib0 = sum(h.launch_count() for h in par.handles)
+    barrier()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        res = par.run(psi, r, v, tol=1e-6)
+        fin = par.final_state()
+        psi_out = fin.psi.cpu().numpy().view(np.complex128).reshape(psi.shape)
+        r_out = fin.r.cpu().numpy()
+        v_out = fin.v.cpu().numpy()
+        e2e_s = time.perf_counter() - t0
+    clocks = clk.summary()
+    launches = sum(h.launch_count() for h in par.handles) - n_lib0 + net.launches
+    par.close()
+    # accuracy against the plain FP64 sequential run over the same time
+    with pkg.He4Step(p) as g64:
+        g64.set_state(psi, r, v)
+        g64.run(S * K, dt)
+        psi64 = g64.get_state()[0]
+        e64 = g64.energy()
+        g64.set_state(psi_out, r_out, v_out)
+        epar = g64.energy()
+    d64, dpar = np.abs(psi64) ** 2, np.abs(psi_out) ** 2
+    sim_ps = S * K * DT_FS * 1e-3
+    return {"form": FORMS["parareal"], "sim_ps": sim_ps, "device_s": res["device_s"], "e2e_s": e2e_s,
+            "iterations": res["iterations"],
+            "converged": res["converged"], "diverged": res["diverged"], "fallback_at": res["fallback_at"],
+            "changes": res["changes"], "fine_steps_executed": res["fine_steps"],
+            "fno": {"training_trajectories": args.fno_traj, "training_steps": args.fno_steps,
+                    "held_out_rel_error_before": before, "held_out_rel_error_after": after,
+                    "train_and_data_s": t_train},
+            "vs_plain_fp64_serial": {"density_rel_l2": float(np.linalg.norm(dpar - d64) / np.linalg.norm(d64)),
+                                     "etot_rel_diff": abs(epar["etot"] - e64["etot"]) / abs(e64["etot"])},
+            "gpu_launches": launches, "clocks": clocks,
+            "e2e_h2d": psi.nbytes + r.nbytes + v.nbytes,
+            "e2e_d2h": psi.nbytes + r.nbytes + v.nbytes}
+
+
 def pin(torch, a):
     t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     return t
 
 
-def kernel_roofline(pkg, g, stream, args):
+def kernel_roofline(pkg, g, stream, args, form):
     """Average duration of the dominant kernel, timed with CUDA events on the
     library's stream, against its algorithmic bytes."""
     L = pkg.load_library()
@@ -297,7 +408,7 @@ def kernel_roofline(pkg, g, stream, args):
     traffic = None
     prof = os.path.join(ROOT, "profiles", "fft_passes_c3.json")
     if args.config == "c3" and os.path.exists(prof):
-        key = kname if args.form == "fp64" else f"{kname}:{args.form}"
+        key = kname if form == "fp64" else f"{kname}:{form}"
         traffic = json.load(open(prof))["traffic_bytes_per_launch"].get(key)
     return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src,
@@ -386,7 +497,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
-    ap.add_argument("--form", default="fp32", choices=sorted(FORMS))
+    ap.add_argument("--form", default="parareal", choices=sorted(FORMS))
+    ap.add_argument("--fno-traj", type=int, default=24, help="training trajectories of the FNO (parareal form)")
+    ap.add_argument("--fno-steps", type=int, default=600, help="training steps of the FNO (parareal form)")
     ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other forms on the same workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")

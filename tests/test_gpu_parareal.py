@@ -113,7 +113,7 @@ def test_trained_fno_beats_identity_coarse_step(pkg, setup):
     for name, G in (("fno", s["enc"]), ("identity", pkg.parareal.IdentityCoarse(STEPS * s["dt"]))):
         par = pkg.parareal.Parareal(s["p"], SLICES, STEPS, s["dt"], G)
         try:
-            par.run(s["psi"], s["r"], s["v"], tol=0.0, max_iter=1)
+            par.run(s["psi"], s["r"], s["v"], tol=0.0, max_iter=1, fallback=False)
             errs[name] = max(rel(boundary_psi(par, n), s["ref"][n - 1]) for n in range(1, SLICES + 1))
         finally:
             par.close()
