@@ -76,12 +76,16 @@ struct AxisPlan {
 struct FftPlan {
   int nx = 0, ny = 0, nz = 0, nxh = 0;
   AxisPlan ax, ay, az;
-  int wy = 8, wz = 8;   // pencils per CTA in the y and z passes
-  int px = 8;           // complex pencils (= row pairs) per CTA in the x pass
+  int wy = 8, wz = 8;   // pencils per CTA in the y and z passes (generic path)
+  int px = 8;           // complex pencils (= row pairs) per CTA in the x pass (generic path)
+  int n1[3] = {0, 0, 0};  // four-step split N = N1 * N2 per axis (register path)
 };
 
 int fft_plan_init(FftPlan &P, int nx, int ny, int nz);
 void fft_plan_free(FftPlan &P);
+// tile shapes t = {n1x, n1y, n1z, px, wy, wz} (fft.cu)
+int fft_set_tiles(FftPlan &P, const int *t);
+void fft_get_tiles(const FftPlan &P, int *t);
 
 // ---------------------------------------------------------------------------
 // stencil weights (centre row of the Bickley matrix, times 1/h^order)
@@ -282,6 +286,8 @@ int step_pc(Handle *h, double dt, double *dres);
 // results of step s land in dres[12 s .. 12 s + 11]
 int run_pc_graphs(Handle *h, int n, double dt, double *dres);
 void free_graphs(Handle *h);
+StepState get_step_state(const Handle *h, double dt);
+void set_step_state(Handle *h, const StepState &s);
 int compute_energy(Handle *h, he4_energies *e);
 int compute_diagnostics(Handle *h, int n4, double *host_out);
 int compute_den(Handle *h);

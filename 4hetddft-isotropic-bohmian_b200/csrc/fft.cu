@@ -18,6 +18,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include <cuda_pipeline.h>
 
@@ -380,6 +381,29 @@ static size_t smem_yz(int n, int W) {
   return sizeof(double2) * (2 * (size_t)n * W + n) + sizeof(long) * W + 2 * sizeof(int) * W;
 }
 
+// The dynamic shared memory limits of the generic-path kernels are
+// process-wide; they only ever grow, to the widest tiles any plan uses.
+static int generic_attrs(const FftPlan &P) {
+  static std::mutex mu;
+  static size_t max_x = 0, max_y = 0, max_z = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (smem_x(P) > max_x) {
+    max_x = smem_x(P);
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_x));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_x));
+  }
+  if (smem_yz(P.ny, P.wy) > max_y) {
+    max_y = smem_yz(P.ny, P.wy);
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_y));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_y));
+  }
+  if (smem_yz(P.nz, P.wz) > max_z) {
+    max_z = smem_yz(P.nz, P.wz);
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_z));
+  }
+  return HE4_OK;
+}
+
 int fft_plan_init(FftPlan &P, int nx, int ny, int nz) {
   P.nx = nx;
   P.ny = ny;
@@ -391,18 +415,62 @@ int fft_plan_init(FftPlan &P, int nx, int ny, int nz) {
   P.px = tile_width(nx);
   P.wy = tile_width(ny);
   P.wz = tile_width(nz);
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x(P)));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x(P)));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(ny, P.wy)));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(ny, P.wy)));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_yz(nz, P.wz)));
+  HE4_TRY(generic_attrs(P));
   const int ns[3] = {nx, ny, nz};
-  for (int n : ns)
-    if (reg_ok(n)) {
-      HE4_REG_SWITCH(n, HE4_TRY((reg_attrs<NN, double2>())));
-      HE4_REG_SWITCH(n, HE4_TRY((reg_attrs<NN, float2>())));
+  for (int a = 0; a < 3; a++) {
+    const int n = ns[a];
+    P.n1[a] = reg_ok(n) ? reg_default_n1(n) : 0;
+    if (!reg_ok(n)) continue;
+    for (int n1 = 2; n1 <= 16; n1 *= 2) {
+      if (!reg_n1_ok(n, n1)) continue;
+      HE4_REG_SWITCH(n, n1, HE4_TRY((reg_attrs<NN, N1_, double2>())));
+      HE4_REG_SWITCH(n, n1, HE4_TRY((reg_attrs<NN, N1_, float2>())));
     }
+  }
   return HE4_OK;
+}
+
+// Tile shapes: t = {n1 x, n1 y, n1 z, px, wy, wz}.  n1 applies to register
+// path axes (0 = default split), px / wy / wz (pencils per CTA, multiples of
+// 8 in [8, 32]) to generic-path axes; entries for the other path are ignored.
+int fft_set_tiles(FftPlan &P, const int *t) {
+  const int ns[3] = {P.nx, P.ny, P.nz};
+  int n1[3];
+  for (int a = 0; a < 3; a++) {
+    n1[a] = 0;
+    if (!reg_ok(ns[a])) continue;
+    n1[a] = t[a] ? t[a] : reg_default_n1(ns[a]);
+    if (!reg_n1_ok(ns[a], n1[a])) {
+      set_error("axis %d: no register FFT split %d x %d", a, n1[a], ns[a] / n1[a]);
+      return HE4_E_ARG;
+    }
+  }
+  FftPlan Q = P;
+  Q.px = reg_ok(P.nx) ? P.px : t[3];
+  Q.wy = reg_ok(P.ny) ? P.wy : t[4];
+  Q.wz = reg_ok(P.nz) ? P.wz : t[5];
+  const int ws[3] = {Q.px, Q.wy, Q.wz};
+  for (int a = 0; a < 3; a++)
+    if (ws[a] < 8 || ws[a] > 32 || ws[a] % 8) {
+      set_error("tile width %d is not a multiple of 8 in [8, 32]", ws[a]);
+      return HE4_E_ARG;
+    }
+  const size_t lim = 200 * 1024;
+  if (smem_x(Q) > lim || smem_yz(Q.ny, Q.wy) > lim || smem_yz(Q.nz, Q.wz) > lim) {
+    set_error("tile widths need more than %zu bytes of shared memory", lim);
+    return HE4_E_ARG;
+  }
+  HE4_TRY(generic_attrs(Q));
+  for (int a = 0; a < 3; a++) Q.n1[a] = n1[a];
+  P = Q;
+  return HE4_OK;
+}
+
+void fft_get_tiles(const FftPlan &P, int *t) {
+  for (int a = 0; a < 3; a++) t[a] = P.n1[a];
+  t[3] = P.px;
+  t[4] = P.wy;
+  t[5] = P.wz;
 }
 
 void fft_plan_free(FftPlan &P) {
@@ -438,13 +506,13 @@ static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *cons
       a.cout[i] = reinterpret_cast<C2 *>(cout[i]);
     }
   }
-  HE4_REG_SWITCH(P.nx, {
-    constexpr int Pp = kRegThreads / RegShape<NN>::N1;
+  HE4_REG_SWITCH(P.nx, P.n1[0], {
+    constexpr int Pp = kRegThreads / N1_;
     dim3 grid((unsigned)((nrow + 2 * Pp - 1) / (2 * Pp)), nb);
     if (inverse)
-      k_xc2r_reg<NN, C2><<<grid, kRegThreads, smem_x_reg<NN, C2>(), h->stream>>>(a);
+      k_xc2r_reg<NN, N1_, C2><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
     else
-      k_xr2c_reg<NN, C2><<<grid, kRegThreads, smem_x_reg<NN, C2>(), h->stream>>>(a);
+      k_xr2c_reg<NN, N1_, C2><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
   });
   HE4_LAUNCHED(h);
   return HE4_OK;
@@ -513,15 +581,15 @@ static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse
   a.box = (axis == 1) ? box : nullptr;
   a.nz = P.nz;
   for (int i = 0; i < nb; i++) a.buf[i] = reinterpret_cast<C2 *>(buf[i]);
-  HE4_REG_SWITCH(len, {
-    constexpr int W = kRegThreads / RegShape<NN>::N1;
+  HE4_REG_SWITCH(len, P.n1[axis], {
+    constexpr int W = kRegThreads / N1_;
     map.W = W;
     a.map = map;
     dim3 grid((unsigned)((total + W - 1) / W), nb);
     if (inverse)
-      k_yz_reg<NN, true, C2><<<grid, kRegThreads, smem_yz_reg<NN, C2>(), h->stream>>>(a);
+      k_yz_reg<NN, N1_, true, C2><<<grid, kRegThreads, smem_yz_reg<NN, N1_, C2>(), h->stream>>>(a);
     else
-      k_yz_reg<NN, false, C2><<<grid, kRegThreads, smem_yz_reg<NN, C2>(), h->stream>>>(a);
+      k_yz_reg<NN, N1_, false, C2><<<grid, kRegThreads, smem_yz_reg<NN, N1_, C2>(), h->stream>>>(a);
   });
   HE4_LAUNCHED(h);
   return HE4_OK;
@@ -653,14 +721,14 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
     const long total = (long)P.nxh * P.ny;
     bool single = true;
     for (int i = 0; i < nb; i++) single = single && (a.g[i].nout == 1);
-    HE4_REG_SWITCH(P.nz, {
-      constexpr int W = kRegThreads / RegShape<NN>::N1;
+    HE4_REG_SWITCH(P.nz, P.n1[2], {
+      constexpr int W = kRegThreads / N1_;
       a.map.W = W;
       dim3 grid(nb, (unsigned)((total + W - 1) / W));
       if (single)
-        k_zconv_reg<NN, true, C2><<<grid, kRegThreads, smem_zconv<NN, true, C2>(), h->stream>>>(a);
+        k_zconv_reg<NN, N1_, true, C2><<<grid, kRegThreads, smem_zconv<NN, N1_, true, C2>(), h->stream>>>(a);
       else
-        k_zconv_reg<NN, false, C2><<<grid, kRegThreads, smem_zconv<NN, false, C2>(), h->stream>>>(a);
+        k_zconv_reg<NN, N1_, false, C2><<<grid, kRegThreads, smem_zconv<NN, N1_, false, C2>(), h->stream>>>(a);
     });
     HE4_LAUNCHED(h);
   }
@@ -730,10 +798,11 @@ static int zsum_reg(Handle *h, int nterm, const ZTerm *terms, double2 *out) {
   }
   a.out = reinterpret_cast<C2 *>(out);
   const long total = (long)P.nxh * P.ny;
-  HE4_REG_SWITCH(P.nz, {
-    constexpr int W = kRegThreads / RegShape<NN>::N1;
+  HE4_REG_SWITCH(P.nz, P.n1[2], {
+    constexpr int W = kRegThreads / N1_;
     a.map.W = W;
-    k_zsum_reg<NN, C2><<<(unsigned)((total + W - 1) / W), kRegThreads, smem_zsum<NN, C2>(), h->stream>>>(a);
+    k_zsum_reg<NN, N1_, C2><<<(unsigned)((total + W - 1) / W), kRegThreads, smem_zsum<NN, N1_, C2>(),
+                             h->stream>>>(a);
   });
   HE4_LAUNCHED(h);
   return HE4_OK;

@@ -13,19 +13,20 @@ namespace he4 {
 constexpr int kRegThreads = 256;
 constexpr int kRegBatch = 8;
 
-template <int N>
-struct RegShape;
-template <>
-struct RegShape<16> { static constexpr int N1 = 4; };
-template <>
-struct RegShape<32> { static constexpr int N1 = 4; };
-template <>
-struct RegShape<64> { static constexpr int N1 = 8; };
-template <>
-struct RegShape<128> { static constexpr int N1 = 8; };
-template <>
-struct RegShape<256> { static constexpr int N1 = 16; };
-
+// Four-step split N = N1 * N2 of the register path: N2 must be a multiple
+// of N1 and both must have a codelet (2, 4, 8, 16).  The first choice is the
+// default; the tile autotuner may pick the other.
+inline int reg_default_n1(int n) { return n == 64 ? 8 : n == 128 ? 8 : n == 256 ? 16 : 4; }
+inline bool reg_n1_ok(int n, int n1) {
+  switch (n) {
+    case 16: return n1 == 4 || n1 == 2;
+    case 32: return n1 == 4 || n1 == 2;
+    case 64: return n1 == 8 || n1 == 4;
+    case 128: return n1 == 8;
+    case 256: return n1 == 16;
+    default: return false;
+  }
+}
 inline bool reg_ok(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256; }
 
 // pencil enumeration for the y and z passes over a half spectrum
@@ -114,28 +115,28 @@ __device__ __forceinline__ void load_tw_n(C2 *s_tw, const C2 *__restrict__ g_tw)
   for (int t = threadIdx.x; t < N; t += blockDim.x) s_tw[t] = g_tw[t];
 }
 
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 inline size_t smem_yz_reg() {
-  constexpr int N1 = RegShape<N>::N1, W = kRegThreads / N1;
+  constexpr int W = kRegThreads / N1;
   return sizeof(C2) * ((size_t)N * W + N) + (sizeof(long) + 2 * sizeof(int)) * W;
 }
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 inline size_t smem_x_reg() {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kRegThreads / N1;
+  constexpr int N2 = N / N1, P = kRegThreads / N1;
   return sizeof(C2) * ((size_t)P * N2 * (N1 + 1) + N);
 }
-template <int N, bool SINGLE, typename C2>
+template <int N, int N1, bool SINGLE, typename C2>
 inline size_t smem_zconv() {
   using T = typename regfft::Re<C2>::type;
-  constexpr int N1 = RegShape<N>::N1, W = kRegThreads / N1;
+  constexpr int W = kRegThreads / N1;
   return sizeof(C2) * ((size_t)N * W + N) + sizeof(T) * (SINGLE ? 1 : 2) * (size_t)N * W +
          (sizeof(long) + 2 * sizeof(int)) * W;
 }
 
 // in-place transform of strided pencils (y pass, or z without multiply)
-template <int N, bool INV, typename C2>
+template <int N, int N1, bool INV, typename C2>
 __global__ void __launch_bounds__(kRegThreads) k_yz_reg(YRegArgs<C2> a) {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kRegThreads / N1;
+  constexpr int N2 = N / N1, W = kRegThreads / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
   long *offs = reinterpret_cast<long *>(tw + N);
@@ -176,10 +177,10 @@ __global__ void __launch_bounds__(kRegThreads) k_yz_reg(YRegArgs<C2> a) {
 // copied to shared memory with cp.async one output ahead (the first ones
 // before the input is even loaded), so their latency hides behind the FFT
 // work.  SINGLE: one output, multiplied in place (fewer registers).
-template <int N, bool SINGLE, typename C2>
+template <int N, int N1, bool SINGLE, typename C2>
 __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
   using T = typename regfft::Re<C2>::type;
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kRegThreads / N1;
+  constexpr int N2 = N / N1, W = kRegThreads / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
   T *Ks = reinterpret_cast<T *>(tw + N);  // [SINGLE ? 1 : 2][N][W]
@@ -255,10 +256,10 @@ __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
 }
 
 // x pass R2C: two real rows per complex pencil, Hermitian split
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
   using T = typename regfft::Re<C2>::type;
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
+  constexpr int N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + P * SP;
   load_tw_n<N>(tw, a.tw);
@@ -293,9 +294,9 @@ __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
 }
 
 // x pass C2R: Hermitian extension of two half spectra, inverse, two rows
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
+  constexpr int N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + P * SP;
   load_tw_n<N>(tw, a.tw);
@@ -364,17 +365,17 @@ struct ZSumArgs {
   C2 *out;
 };
 
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 inline size_t smem_zsum() {
   using T = typename regfft::Re<C2>::type;
-  constexpr int N1 = RegShape<N>::N1, W = kRegThreads / N1;
+  constexpr int W = kRegThreads / N1;
   return sizeof(C2) * ((size_t)N * W + N) + sizeof(T) * (size_t)N * W + sizeof(long) * W;
 }
 
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 __global__ void __launch_bounds__(kRegThreads) k_zsum_reg(ZSumArgs<C2> a) {
   using T = typename regfft::Re<C2>::type;
-  constexpr int N1 = RegShape<N>::N1, N2 = N / N1, W = kRegThreads / N1;
+  constexpr int N2 = N / N1, W = kRegThreads / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
   T *Ks = reinterpret_cast<T *>(tw + N);  // [N][W]
@@ -432,33 +433,45 @@ __global__ void __launch_bounds__(kRegThreads) k_zsum_reg(ZSumArgs<C2> a) {
   }
 }
 
-template <int N, typename C2>
+template <int N, int N1, typename C2>
 inline int reg_attrs() {
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zsum_reg<N, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_zsum<N, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_yz_reg<N, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_yz_reg<N, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_zconv<N, true, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_zconv<N, false, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_x_reg<N, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_x_reg<N, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zsum_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zsum<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_yz_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_yz_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zconv<N, N1, true, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zconv<N, N1, false, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_x_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_x_reg<N, N1, C2>()));
   return HE4_OK;
 }
 
-// run the statement with NN = n (n one of the register-path lengths)
-#define HE4_REG_SWITCH(n, ...)                                  \
-  switch (n) {                                                  \
-    case 16: { constexpr int NN = 16; __VA_ARGS__; } break;     \
-    case 32: { constexpr int NN = 32; __VA_ARGS__; } break;     \
-    case 64: { constexpr int NN = 64; __VA_ARGS__; } break;     \
-    case 128: { constexpr int NN = 128; __VA_ARGS__; } break;   \
-    default: { constexpr int NN = 256; __VA_ARGS__; } break;    \
-  }
+// run the statement with NN = n and N1_ = n1 (a pair reg_n1_ok accepts)
+#define HE4_REG_CASE(a, b, ...)                   \
+  if (n_ == a && n1_ == b) {                      \
+    constexpr int NN = a, N1_ = b;                \
+    __VA_ARGS__;                                  \
+  } else
+#define HE4_REG_SWITCH(n, n1, ...)                \
+  do {                                            \
+    const int n_ = (n), n1_ = (n1);               \
+    HE4_REG_CASE(16, 4, __VA_ARGS__)              \
+    HE4_REG_CASE(16, 2, __VA_ARGS__)              \
+    HE4_REG_CASE(32, 4, __VA_ARGS__)              \
+    HE4_REG_CASE(32, 2, __VA_ARGS__)              \
+    HE4_REG_CASE(64, 8, __VA_ARGS__)              \
+    HE4_REG_CASE(64, 4, __VA_ARGS__)              \
+    HE4_REG_CASE(128, 8, __VA_ARGS__)             \
+    HE4_REG_CASE(256, 16, __VA_ARGS__) {          \
+      set_error("no register FFT for %d = %d x %d", n_, n1_, n_ / (n1_ ? n1_ : 1)); \
+      return HE4_E_UNSUPPORTED;                   \
+    }                                             \
+  } while (0)
 
 }  // namespace he4

@@ -374,7 +374,7 @@ int step_pc(Handle *h, double dt, double *dres) {
 // ---------------------------------------------------------------------------
 // CUDA graphs of the PC step
 // ---------------------------------------------------------------------------
-static StepState get_step_state(const Handle *h, double dt) {
+StepState get_step_state(const Handle *h, double dt) {
   StepState s;
   memset(&s, 0, sizeof(s));
   s.psi = h->psi;
@@ -397,7 +397,7 @@ static StepState get_step_state(const Handle *h, double dt) {
   return s;
 }
 
-static void set_step_state(Handle *h, const StepState &s) {
+void set_step_state(Handle *h, const StepState &s) {
   h->psi = s.psi;
   h->ctmp = s.ctmp;
   for (int i = 0; i < 3; i++) {

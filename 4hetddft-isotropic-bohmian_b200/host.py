@@ -54,6 +54,20 @@ def load_library():
     L.he4_get_kernel.argtypes = [vp, i32, dp]
     L.he4_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.he4_device_ptr.argtypes = [vp, i32, C.POINTER(vp)]
+    ip = C.POINTER(C.c_int32)
+    L.he4_set_tiles.argtypes = [vp, ip]
+    L.he4_get_tiles.argtypes = [vp, ip]
+    L.he4_tune.argtypes = [vp, i32, dp, ip]
+    L.he4_batch_create.argtypes = [i32, vp, C.POINTER(vp)]
+    L.he4_batch_destroy.argtypes = [vp]
+    L.he4_batch_destroy.restype = None
+    L.he4_batch_size.argtypes = [vp]
+    L.he4_batch_member.argtypes = [vp, i32]
+    L.he4_batch_member.restype = vp
+    L.he4_batch_tune.argtypes = [vp, i32, ip, dp]
+    L.he4_batch_run.argtypes = [vp, i32, C.c_double, dp, dp]
+    L.he4_batch_launch_count.argtypes = [vp]
+    L.he4_batch_launch_count.restype = C.c_int64
     L.he4_launch_count.argtypes = [vp]
     L.he4_launch_count.restype = C.c_int64
     L.he4_strerror.argtypes = [C.c_int]
@@ -84,19 +98,39 @@ def params_default():
 class He4Step:
     """Device-resident time step of one droplet + impurity system."""
 
-    def __init__(self, params):
+    def __init__(self, params, _borrowed=None):
         L = load_library()
         self.p = params
-        self._h = C.c_void_p()
-        _check(L.he4_create(C.byref(params), C.byref(self._h)), "he4_create")
+        self._owned = _borrowed is None
+        if _borrowed is None:
+            self._h = C.c_void_p()
+            _check(L.he4_create(C.byref(params), C.byref(self._h)), "he4_create")
+        else:
+            self._h = C.c_void_p(_borrowed)
         self.shape = (params.nz, params.ny, params.nx)
         self.hshape = (params.nz, params.ny, params.nx // 2 + 1)
         self.npar = params.n_par
 
     def close(self):
-        if self._h:
+        if self._h and self._owned:
             load_library().he4_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
+
+    def tiles(self):
+        t = (C.c_int32 * 6)()
+        _check(load_library().he4_get_tiles(self._h, t), "he4_get_tiles")
+        return list(t)
+
+    def set_tiles(self, tiles):
+        t = (C.c_int32 * 6)(*tiles)
+        _check(load_library().he4_set_tiles(self._h, t), "he4_set_tiles")
+
+    def tune(self, reps=3):
+        """he4_tune: returns (tiles, ms per field evaluation)."""
+        t = (C.c_int32 * 6)()
+        ms = C.c_double()
+        _check(load_library().he4_tune(self._h, reps, C.byref(ms), t), "he4_tune")
+        return list(t), ms.value
 
     def __del__(self):
         try:
@@ -205,3 +239,56 @@ class He4Step:
 
     def launch_count(self):
         return int(load_library().he4_launch_count(self._h))
+
+
+class He4Batch:
+    """Batched ensemble of independent systems (he4_batch_*): members are
+    He4Step views that do not own their handles."""
+
+    def __init__(self, params_list):
+        L = load_library()
+        n = len(params_list)
+        arr = (abi.He4Params * n)(*params_list)
+        self._b = C.c_void_p()
+        _check(L.he4_batch_create(n, arr, C.byref(self._b)), "he4_batch_create")
+        self.members = [He4Step(params_list[i], _borrowed=L.he4_batch_member(self._b, i)) for i in range(n)]
+
+    def __len__(self):
+        return len(self.members)
+
+    def close(self):
+        if self._b:
+            for m in self.members:
+                m.close()
+            load_library().he4_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def tune(self, reps=3):
+        n = len(self.members)
+        t = (C.c_int32 * (6 * n))()
+        ms = np.zeros(n)
+        _check(load_library().he4_batch_tune(self._b, reps, t, _dp(ms)), "he4_batch_tune")
+        return np.array(list(t), dtype=np.int32).reshape(n, 6), ms
+
+    def run(self, nsteps, deltat):
+        """Advances every member; returns (err_max [n][3], means [n][9])."""
+        n = len(self.members)
+        e = np.zeros((n, 3))
+        m = np.zeros((n, 9))
+        _check(load_library().he4_batch_run(self._b, nsteps, deltat, _dp(e), _dp(m)), "he4_batch_run")
+        return e, m
+
+    def launch_count(self):
+        return load_library().he4_batch_launch_count(self._b)

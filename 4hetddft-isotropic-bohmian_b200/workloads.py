@@ -129,3 +129,25 @@ def family_member(name, seed):
     psi = droplet_psi(p, cfg["n4"])
     rimp, vimp = particles(cfg["npar"], seed, speed, center=tuple(center))
     return p, psi, rimp, vimp
+
+
+def ensemble_member(i, seed0=0, npar=1024):
+    """Member i of the batched ensemble: N log-uniform in [200, 3000], the
+    smallest grid of 64^3, 96^3, 128^3 whose spacing 2.5 R / n stays within
+    [0.4, 0.6] A (the spacing clamped to that range), impurity speed uniform
+    in [50, 300] m/s, npar test particles 2 A off centre.  Returns (params,
+    psi, rimp, vimp, n4)."""
+    rng = np.random.Generator(np.random.PCG64(seed0 + i))
+    n4 = int(round(math.exp(rng.uniform(math.log(200.0), math.log(3000.0)))))
+    R = 2.22 * n4 ** (1.0 / 3.0)
+    n = 128
+    for cand in (64, 96, 128):
+        if 2.5 * R / cand <= 0.6:
+            n = cand
+            break
+    h = min(0.6, max(0.4, 2.5 * R / n))
+    speed = rng.uniform(50.0, 300.0)
+    p = make_params(n, h, npar)
+    psi = droplet_psi(p, n4)
+    rimp, vimp = particles(npar, seed0 + i, speed)
+    return p, psi, rimp, vimp, n4

@@ -210,6 +210,39 @@ int he4_device_ptr(he4_handle *h, int32_t which, void **ptr);
  * kernels inside the graph). */
 int64_t he4_launch_count(he4_handle *h);
 
+/* Tile shapes of the FFT passes: tiles = {n1 x, n1 y, n1 z, px, wy, wz}.
+ * For axis lengths 16..256 (powers of two) n1 is the four-step split
+ * N = n1 * (N / n1) of the register path (0 = default); for the other
+ * lengths px / wy / wz are the pencils per CTA (multiples of 8 in [8, 32])
+ * of the x, y and z passes.  Setting drops the handle's captured graphs. */
+int he4_set_tiles(he4_handle *h, const int32_t tiles[6]);
+int he4_get_tiles(he4_handle *h, int32_t tiles[6]);
+/* Autotuner: coordinate search over the tile shapes of the three axes,
+ * each candidate timed (CUDA events) as `reps` mean-field evaluations of
+ * the current state; the fastest shapes are applied and returned. */
+int he4_tune(he4_handle *h, int32_t reps, double *best_ms, int32_t tiles[6]);
+
+/* Batched ensemble: n independent systems (grids may differ; one device)
+ * advanced together, one CUDA graph launch per ensemble PC step (every
+ * member's step is a parallel branch of the graph).  Members are ordinary
+ * handles: he4_set_state / he4_get_state / he4_energy on
+ * he4_batch_member(b, i) work as for any handle and are ordered after the
+ * ensemble's work.  he4_batch_tune tunes one member per distinct grid and
+ * applies its shapes to the others (tiles [n][6], ms [n], either may be
+ * NULL).  he4_batch_run advances every member by nsteps (RK-Gill starter
+ * first where a member needs it) and returns per member the largest
+ * errHe/errimp/errvimp of the run (err_max [n][3]) and the last step's
+ * means ([n][9]); HE4_E_NONFINITE names the first member that went
+ * non-finite. */
+typedef struct he4_batch he4_batch;
+int he4_batch_create(int32_t n, const he4_params *params, he4_batch **out);
+void he4_batch_destroy(he4_batch *b);
+int32_t he4_batch_size(const he4_batch *b);
+he4_handle *he4_batch_member(he4_batch *b, int32_t i);
+int he4_batch_tune(he4_batch *b, int32_t reps, int32_t *tiles, double *ms);
+int he4_batch_run(he4_batch *b, int32_t nsteps, double deltat, double *err_max, double *means);
+int64_t he4_batch_launch_count(const he4_batch *b);
+
 const char *he4_strerror(int code);
 const char *he4_last_error(void);
 
