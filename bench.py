@@ -145,8 +145,8 @@ def replica_throughput(world, sim_ps_per_rank, seconds_max):
 FORMS = {"fp64": "plain FP64", "fp32": "FP32 convolutions (FP32 half spectra, kernels and twiddles; "
                                          "FP64 real grids, psi update, reductions and trajectories)",
          "parareal": "learned parareal: FNO coarse step (64^3, width 32, 12 modes/axis, 4 layers, BF16 weights) "
-                     "+ FP32-convolution PC fine propagator over 16 slices of 50 fs, sequential fallback"}
-PARAREAL_SLICES, PARAREAL_STEPS = 16, 50
+                     "+ FP32-convolution PC fine propagator over 6 slices of 50 fs, sequential fallback"}
+PARAREAL_SLICES, PARAREAL_STEPS = 6, 50
 
 
 def form_params(pkg, p, form):
@@ -228,6 +228,9 @@ def gpu_arm(args):
         ms_max = par["ms_per_step"]
         launches = par["gpu_launches"]
         clocks = par["clocks"]
+
+    if args.ensemble > 0 and world == 1:
+        forms["ensemble"] = ensemble_form(pkg, args, local, barrier)
 
     # ---- end to end through the per-step C ABI with host buffers:
     # he4_set_state (pinned host -> device), 3 he4_step_rk + (K-3)
@@ -382,6 +385,67 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
             "e2e_d2h": psi.nbytes + r.nbytes + v.nbytes}
 
 
+def ensemble_form(pkg, args, local, barrier):
+    """The batched ensemble: 64 members (N log-uniform in [200, 3000],
+    grids 64^3 / 96^3 / 128^3, 1024 test particles, 50-300 m/s), tile shapes
+    from the autotuner, K ensemble PC steps timed; the same members run one
+    after the other (each through its own he4_run) give the unbatched time."""
+    import torch
+    w = pkg.workloads
+    dt = w.deltat_fs(DT_FS)
+    ms = [w.ensemble_member(i) for i in range(args.ensemble)]
+    params = []
+    for m in ms:
+        m[0].device = local
+        params.append(m[0])
+    grids = {}
+    for m in ms:
+        grids[m[0].nx] = grids.get(m[0].nx, 0) + 1
+    t0 = time.perf_counter()
+    b = pkg.He4Batch(params)
+    t_create = time.perf_counter() - t0
+    for mem, m in zip(b.members, ms):
+        mem.set_state(m[1], m[2], m[3])
+    t0 = time.perf_counter()
+    tiles, tms = b.tune(reps=3)
+    t_tune = time.perf_counter() - t0
+    b.run(3 + args.warmup, dt)
+    K = args.ensemble_steps
+    barrier()
+    n0 = b.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        err, means = b.run(K, dt)
+        torch.cuda.synchronize(local)
+        e1.record()
+        e1.synchronize()
+    batched_s = e0.elapsed_time(e1) * 1e-3
+    launches = b.launch_count() - n0
+    clocks = clk.summary()
+    # the same members one after the other (unbatched), same tiles and state phase
+    barrier()
+    e0.record()
+    for mem in b.members:
+        mem.run(K, dt)
+    torch.cuda.synchronize(local)
+    e1.record()
+    e1.synchronize()
+    seq_s = e0.elapsed_time(e1) * 1e-3
+    per_grid = {}
+    for t, m in zip(tiles.tolist(), ms):
+        per_grid.setdefault(f"{m[0].nx}^3", t)
+    b.close()
+    sim = args.ensemble * K * DT_FS * 1e-3
+    return {"form": f"batched ensemble of {args.ensemble} systems, one graph launch per ensemble step",
+            "members_per_grid": {f"{k}^3": v for k, v in sorted(grids.items())}, "steps": K,
+            "value": sim / (batched_s / 3600.0), "unit": "simulated ps/hour (sum over members)",
+            "ms_per_ensemble_step": batched_s * 1e3 / K, "unbatched_ms_per_ensemble_step": seq_s * 1e3 / K,
+            "batching_speedup": seq_s / batched_s, "gpu_launches": launches,
+            "tiles_per_grid": per_grid, "create_s": t_create, "tune_s": t_tune, "clocks": clocks}
+
+
 def pin(torch, a):
     t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     return t
@@ -502,6 +566,8 @@ def main():
     ap.add_argument("--fno-steps", type=int, default=600, help="training steps of the FNO (parareal form)")
     ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other forms on the same workload")
+    ap.add_argument("--ensemble", type=int, default=64, help="ensemble members timed beside (0 = skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
