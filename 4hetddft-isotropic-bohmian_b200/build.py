@@ -28,6 +28,9 @@ def _stale():
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(HERE, "..", "include", "he4_tddft.h"))
     deps.append(os.path.join(HERE, "..", "include", "he4_fno.h"))
+    deps += [os.path.join(HERE, "driver", f) for f in DRIVER_SOURCES + ["he4io.hpp"]]
+    if not os.path.exists(DRIVER):
+        return True
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps)
 
@@ -62,7 +65,25 @@ def build(force=False, verbose=False, extra=()):
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_driver(verbose=verbose)
     return LIB
+
+
+DRIVER = os.path.join(HERE, "he4run")
+DRIVER_SOURCES = ["he4io.cpp", "he4run.cpp"]
+
+
+def build_driver(verbose=False):
+    """The C++ host driver (namelist, readenc mode 2, printoutc, time loop),
+    linked against libhe4b200.so next to it."""
+    srcs = [os.path.join(HERE, "driver", f) for f in DRIVER_SOURCES]
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", *srcs, "-o", DRIVER + ".tmp",
+           "-L" + HERE, "-lhe4b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
 
 
 if __name__ == "__main__":
