@@ -614,6 +614,8 @@ static int launch_bench(Handle *h, int which) {
                     {h->spec[0], h->spec[3], h->kalfs, h->renor, -1}};
       return fft_z_conv(h, 3, ops);
     }
+    case 7: return launch_grad(h);
+    case 8: return launch_pot4_merged(h);
     default: set_error("unknown kernel id %d", which); return HE4_E_ARG;
   }
 }
@@ -625,15 +627,18 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
     set_error("invalid arguments");
     return HE4_E_ARG;
   }
-  static const char *names[7] = {"k_fft_z_conv",  "k_fft_y",           "k_fft_x_r2c", "k_fft_x_c2r",
-                                 "k_fft_z_plain", "k_fft_z_conv_nokern", "k_fft_z_conv_3out"};
+  static const char *names[9] = {"k_fft_z_conv",  "k_fft_y",           "k_fft_x_r2c", "k_fft_x_c2r",
+                                 "k_fft_z_plain", "k_fft_z_conv_nokern", "k_fft_z_conv_3out", "k_grad",
+                                 "k_pot4_merged"};
   const double H = (double)h->H, N = (double)h->N;
   // algorithmic bytes: read input once, write output once (+ the real
   // kernel); c and k are the sizes of a spectrum and a kernel element
   const double c = h->fp32 ? 8 : 16, k = h->fp32 ? 4 : 8;
-  const double bytes[7] = {c * H + k * H + c * H, 2 * c * H, 8 * N + c * H, c * H + 8 * N,
-                           2 * c * H,             2 * c * H, c * H + 3 * (k * H + c * H)};
-  if (which < 0 || which > 6) {
+  const double bytes[9] = {c * H + k * H + c * H, 2 * c * H, 8 * N + c * H, c * H + 8 * N,
+                           2 * c * H,             2 * c * H, c * H + 3 * (k * H + c * H),
+                           // stencils: den in, three gradients out; lin, den, dencg, h0..h2 in, pot4 out
+                           4 * 8 * N,             7 * 8 * N};
+  if (which < 0 || which > 8) {
     set_error("unknown kernel id %d", which);
     return HE4_E_ARG;
   }
@@ -651,6 +656,10 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   HE4_TRY(rc);
+  // the timed launches overwrite evaluation buffers: the next step
+  // evaluates the field of its state again
+  h->field_valid = 0;
+  h->split_valid = 0;
   *ms_per_launch = ms / reps;
   *bytes_per_launch = bytes[which];
   if (name && name_len > 0) {

@@ -267,6 +267,9 @@ int field_poten(Handle *h, bool split, double *pot4);
 // reads it (a time step's need).  field_forces recomputes just the field.
 int field_forceimp(Handle *h, bool full);
 int field_forces(Handle *h, bool full);
+// the stencil passes of an evaluation (also timed by he4_bench_kernel)
+int launch_grad(Handle *h);
+int launch_pot4_merged(Handle *h);
 // potenimp + poten + forceimp; marks the fields valid.  split = false takes
 // the merged form when the z length allows it.
 int field_all(Handle *h, bool split = false);

@@ -21,12 +21,154 @@ __global__ void k_grad(const double *__restrict__ f, double *dx, double *dy, dou
   dz[t] = stencil_axis(f, st.w1[2], st.m, g, i, j, k, 2);
 }
 
-// ---------------------------------------------------------------------------
-// poten pointwise pieces
-// ---------------------------------------------------------------------------
+// The same stencils for a compile-time half width M, one CTA of 32 x 8
+// threads marching over ZB consecutive z planes of its (x, y) tile: the z
+// taps come from a register queue of each thread's column (ZB + 2M loads
+// instead of ZB (2M + 1)), the x and y taps from a shared-memory copy of the
+// plane's tile with its periodic halo (about 2 loads per point instead of
+// 4M).  Every tap is summed in the order of stencil_axis, so the results are
+// those of the one-plane kernels.
+constexpr int kZB = 8;
+
 struct OtArgs {
   double cp4, cpp4, den0s, h2o2m4, alphas, c_solid, beta, den_m;
 };
+
+// periodic index for i in [-n, 2n)
+__device__ __forceinline__ int wrap2(int i, int n) { return i < 0 ? i + n : (i >= n ? (i >= 2 * n ? i - 2 * n : i - n) : i); }
+
+// column values k0-M .. k0+ZB-1+M of f at (i, j)
+template <int M, int ZB>
+__device__ __forceinline__ void load_column(const double *__restrict__ f, const Geo &g, int i, int j, int k0,
+                                            double (&q)[ZB + 2 * M]) {
+  const double *col = f + (size_t)j * g.nx + i;
+  const size_t ps = (size_t)g.ny * g.nx;
+#pragma unroll
+  for (int u = 0; u < ZB + 2 * M; u++) q[u] = __ldg(col + (size_t)wrap2(k0 - M + u, g.nz) * ps);
+}
+
+// Plane k of f into the tile s[8 + 2 HY][32 + 2 HX] around (i0, j0): the
+// centre cell of each thread (`centre` when it holds it, from global memory
+// otherwise), an x halo of HX cells on both sides of each row and a y halo
+// of HY rows above and below each column, all periodic.  Corners are not
+// filled (the stencils are one-dimensional).
+template <int HX, int HY>
+__device__ __forceinline__ void fill_tile(const double *__restrict__ f, const Geo &g, int i0, int j0, int k,
+                                          bool have, double centre, double (*s)[32 + 2 * HX]) {
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const double *plane = f + (size_t)k * g.ny * g.nx;
+  const int gi = wrap2(i0 + tx, g.nx), gj = wrap2(j0 + ty, g.ny);
+  s[ty + HY][tx + HX] = have ? centre : __ldg(plane + (size_t)gj * g.nx + gi);
+  if (HX > 0 && tx < HX) {
+    s[ty + HY][tx] = __ldg(plane + (size_t)gj * g.nx + wrap2(i0 - HX + tx, g.nx));
+    s[ty + HY][tx + 32 + HX] = __ldg(plane + (size_t)gj * g.nx + wrap2(i0 + 32 + tx, g.nx));
+  }
+  if (HY > 0 && ty < HY) {
+    s[ty][tx + HX] = __ldg(plane + (size_t)wrap2(j0 - HY + ty, g.ny) * g.nx + gi);
+    s[ty + 8 + HY][tx + HX] = __ldg(plane + (size_t)wrap2(j0 + 8 + ty, g.ny) * g.nx + gi);
+  }
+}
+
+template <int M, int ZB>
+__global__ void __launch_bounds__(256) k_grad_z(const double *__restrict__ f, double *dx, double *dy, double *dz,
+                                                Stencil st, Geo g) {
+  __shared__ double s[8 + 2 * M][32 + 2 * M];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 8, k0 = blockIdx.z * ZB;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in = i < g.nx && j < g.ny;
+  double q[ZB + 2 * M];
+  if (in) load_column<M, ZB>(f, g, i, j, k0, q);
+#pragma unroll
+  for (int zz = 0; zz < ZB; zz++) {
+    const int k = k0 + zz;
+    if (k >= g.nz) break;
+    __syncthreads();
+    fill_tile<M, M>(f, g, i0, j0, k, in, in ? q[zz + M] : 0.0, s);
+    __syncthreads();
+    if (!in) continue;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+#pragma unroll
+    for (int t = -M; t <= M; t++) ax += st.w1[0][t + M] * s[ty + M][tx + M + t];
+#pragma unroll
+    for (int t = -M; t <= M; t++) ay += st.w1[1][t + M] * s[ty + M + t][tx + M];
+#pragma unroll
+    for (int u = -M; u <= M; u++) az += st.w1[2][u + M] * q[zz + M + u];
+    const size_t t = ((size_t)k * g.ny + j) * g.nx + i;
+    dx[t] = ax;
+    dy[t] = ay;
+    dz[t] = az;
+  }
+}
+
+// Every input of the ZB planes of a thread (the z column of h2 with its
+// halo, the centres of h0 and h1, lin, den and dencg) is loaded up front:
+// the kernel is bound by memory latency, not by its (algorithmic) DRAM
+// traffic, so each thread keeps ~30 independent loads in flight and the
+// planes then only wait for the L2-resident tile halos.
+constexpr int kZBp = 4;
+
+template <bool OTC, int M, int ZB>
+__global__ void __launch_bounds__(256) k_pot4_merged_z(const double *__restrict__ lin, const double *__restrict__ den,
+                                                       const double *__restrict__ dencg, const double *__restrict__ h0,
+                                                       const double *__restrict__ h1, const double *__restrict__ h2,
+                                                       double *pot4, Stencil st, Geo g, OtArgs a) {
+  __shared__ double s0[8][32 + 2 * M];   // h0 with its x halo
+  __shared__ double s1[8 + 2 * M][32];   // h1 with its y halo
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 8, k0 = blockIdx.z * ZB;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in = i < g.nx && j < g.ny;
+  const size_t ps = (size_t)g.ny * g.nx;
+  double q[ZB + 2 * M], c0[ZB], c1[ZB], ld[ZB], dd[ZB], dcg[ZB];
+  if (in) {
+    if (OTC) load_column<M, ZB>(h2, g, i, j, k0, q);
+#pragma unroll
+    for (int zz = 0; zz < ZB; zz++) {
+      const size_t t = (size_t)wrap2(k0 + zz, g.nz) * ps + (size_t)j * g.nx + i;
+      if (OTC) {
+        c0[zz] = __ldg(h0 + t);
+        c1[zz] = __ldg(h1 + t);
+      }
+      ld[zz] = __ldg(lin + t);
+      dd[zz] = __ldg(den + t);
+      dcg[zz] = __ldg(dencg + t);
+    }
+  }
+  const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0;
+#pragma unroll
+  for (int zz = 0; zz < ZB; zz++) {
+    const int k = k0 + zz;
+    if (k >= g.nz) break;
+    if (OTC) {
+      __syncthreads();
+      fill_tile<M, 0>(h0, g, i0, j0, k, in, in ? c0[zz] : 0.0, s0);
+      fill_tile<0, M>(h1, g, i0, j0, k, in, in ? c1[zz] : 0.0, s1);
+      __syncthreads();
+    }
+    if (!in) continue;
+    const double d = dd[zz];
+    const double th = tanh(a.beta * (d - a.den_m));
+    const double pen = a.c_solid * (1.0 + th + a.beta * d * (1.0 - th * th));
+    const double dc = dcg[zz];
+    double v = ld[zz] + dc * dc * (a0 + a1 * dc) + pen;
+    if (OTC) {
+      double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+      for (int u = -M; u <= M; u++) d0 += st.w1[0][u + M] * s0[ty][tx + M + u];
+#pragma unroll
+      for (int u = -M; u <= M; u++) d1 += st.w1[1][u + M] * s1[ty + M + u][tx];
+#pragma unroll
+      for (int u = -M; u <= M; u++) d2 += st.w1[2][u + M] * q[zz + M + u];
+      v += (d0 + d1 + d2) * a.h2o2m4 * a.alphas;
+    }
+    pot4[((size_t)k * g.ny + j) * g.nx + i] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// poten pointwise pieces
+// ---------------------------------------------------------------------------
 
 // sto1 = den*dencg*(cp4+cpp4*dencg) (poten.f90:62-64)
 __global__ void k_corr_src(const double *__restrict__ den, const double *__restrict__ dencg, double *out, size_t n,
@@ -162,6 +304,65 @@ __global__ void k_gather(const double *__restrict__ rimp, const double *__restri
 }
 
 // ---------------------------------------------------------------------------
+// stencil launches: the z-marching kernels for npd = 7 and 13 when the grid
+// is deep enough, the one-plane kernels otherwise
+// ---------------------------------------------------------------------------
+// The tiles' periodic indices stay in [-n, 2n) (what wrap2 folds) when
+// nx >= 40, ny >= 16 and nz >= kZB + 2m: the farthest halo cell lies at most
+// 36 cells beyond the last x index and 12 beyond the last y and z index.
+static bool zmarch_ok(const Handle *h) {
+  return (h->st.m == 3 || h->st.m == 6) && h->nx >= 40 && h->ny >= 16 && h->nz >= kZB + 2 * h->st.m;
+}
+
+static dim3 grid_z(const Geo &g, int zb = kZB) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + zb - 1) / zb); }
+
+int launch_grad(Handle *h) {
+  const Geo g = geo(h);
+  if (!zmarch_ok(h))
+    k_grad<<<grid3(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+  else if (h->st.m == 3)
+    k_grad_z<3, kZB><<<grid_z(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+  else
+    k_grad_z<6, kZB><<<grid_z(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+static OtArgs ot_args(const Handle *h);
+
+// pot4 from lin = rtmp[0] and h_i = rtmp[1..3] (merged evaluation)
+int launch_pot4_merged(Handle *h) {
+  const Geo g = geo(h);
+  const OtArgs ot = ot_args(h);
+  const bool otc = (h->p.core4 == HE4_CORE_OTC);
+  const double *h0 = otc ? h->rtmp[1] : nullptr, *h1 = otc ? h->rtmp[2] : nullptr, *h2 = otc ? h->rtmp[3] : nullptr;
+  if (!zmarch_ok(h)) {
+    if (otc)
+      k_pot4_merged<true><<<grid3(g), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h0, h1, h2, h->pot4,
+                                                                h->st, g, ot);
+    else
+      k_pot4_merged<false><<<grid3(g), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h0, h1, h2, h->pot4,
+                                                                 h->st, g, ot);
+  } else if (h->st.m == 3) {
+    if (otc)
+      k_pot4_merged_z<true, 3, kZBp><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h0, h1, h2,
+                                                                          h->pot4, h->st, g, ot);
+    else
+      k_pot4_merged_z<false, 3, kZBp><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h0, h1,
+                                                                           h2, h->pot4, h->st, g, ot);
+  } else {
+    if (otc)
+      k_pot4_merged_z<true, 6, kZBp><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h0, h1, h2,
+                                                                          h->pot4, h->st, g, ot);
+    else
+      k_pot4_merged_z<false, 6, kZBp><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h0, h1,
+                                                                           h2, h->pot4, h->st, g, ot);
+  }
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
+// ---------------------------------------------------------------------------
 // orchestration
 // ---------------------------------------------------------------------------
 static OtArgs ot_args(const Handle *h) {
@@ -218,8 +419,7 @@ static int field_poten_merged(Handle *h) {
     double *out[2] = {h->dencg, h->denalf};
     HE4_TRY(fft_c2r(h, otc ? 2 : 1, sp, out));
   }
-  k_grad<<<grid3(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
-  HE4_LAUNCHED(h);
+  HE4_TRY(launch_grad(h));
   // correlation source, x/y transform kept in spec[5]
   k_corr_src<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->rtmp[0], N, ot);
   HE4_LAUNCHED(h);
@@ -258,13 +458,7 @@ static int field_poten_merged(Handle *h) {
     double *out[1] = {h->rtmp[0]};
     HE4_TRY(fft_c2r(h, 1, sp, out));
   }
-  if (otc)
-    k_pot4_merged<true><<<grid3(g), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, h->rtmp[1], h->rtmp[2],
-                                                              h->rtmp[3], h->pot4, h->st, g, ot);
-  else
-    k_pot4_merged<false><<<grid3(g), block3(), 0, h->stream>>>(h->rtmp[0], h->den, h->dencg, nullptr, nullptr,
-                                                               nullptr, h->pot4, h->st, g, ot);
-  HE4_LAUNCHED(h);
+  HE4_TRY(launch_pot4_merged(h));
   return HE4_OK;
 }
 
@@ -292,8 +486,7 @@ int field_poten(Handle *h, bool split, double *pot4) {
     HE4_TRY(fft_c2r(h, nop, sp, out));
   }
   // derden
-  k_grad<<<grid3(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
-  HE4_LAUNCHED(h);
+  HE4_TRY(launch_grad(h));
   // correlation convolution (poten.f90:62-74)
   k_corr_src<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->rtmp[0], N, ot);
   HE4_LAUNCHED(h);

@@ -192,7 +192,11 @@ int he4_fft_c2r(he4_handle *h, const double *in, double *out);
 /* Measurement hook: launches one kernel of the step `reps` times on the
  * handle's current buffers between two CUDA events on the handle's stream.
  * which: 0 z-pass convolution (FFT_z, kernel multiply, IFFT_z), 1 y pass,
- * 2 x pass R2C, 3 x pass C2R.  They only touch FFT scratch buffers.  Returns
+ * 2 x pass R2C, 3 x pass C2R, 4 plain z pass, 5 z convolution without a
+ * kernel, 6 z convolution with three outputs (these only touch FFT scratch
+ * buffers), 7 the density gradient stencil, 8 the merged pot4 assembly
+ * (these rewrite fields of the current evaluation with the same values, so
+ * call them after a field evaluation).  Returns
  * the mean time per launch, the algorithmic bytes one launch moves (each
  * input read once, each output written once) and the kernel's name. */
 int he4_bench_kernel(he4_handle *h, int32_t which, int32_t reps, double *ms_per_launch,
