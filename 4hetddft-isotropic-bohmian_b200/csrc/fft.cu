@@ -585,11 +585,27 @@ static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse
     constexpr int W = kRegThreads / N1_;
     map.W = W;
     a.map = map;
-    dim3 grid((unsigned)((total + W - 1) / W), nb);
+    const long ntiles = (total + W - 1) / W;
+    // one wave of persistent CTAs: as many as fit on the SMs at once
+    static int per_sm[2] = {0, 0};
+    int &ps = per_sm[inverse ? 1 : 0];
+    if (ps == 0) {
+      int dev = 0, nsm = 0, occ = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (inverse)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_yz_pipe<NN, N1_, true, C2>, kRegThreads,
+                                                      smem_yz_reg<NN, N1_, C2>());
+      else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_yz_pipe<NN, N1_, false, C2>, kRegThreads,
+                                                      smem_yz_reg<NN, N1_, C2>());
+      ps = std::max(1, occ) * std::max(1, nsm);
+    }
+    dim3 grid((unsigned)std::min<long>(ntiles, std::max(1, ps / nb)), nb);
     if (inverse)
-      k_yz_reg<NN, N1_, true, C2><<<grid, kRegThreads, smem_yz_reg<NN, N1_, C2>(), h->stream>>>(a);
+      k_yz_pipe<NN, N1_, true, C2><<<grid, kRegThreads, smem_yz_reg<NN, N1_, C2>(), h->stream>>>(a);
     else
-      k_yz_reg<NN, N1_, false, C2><<<grid, kRegThreads, smem_yz_reg<NN, N1_, C2>(), h->stream>>>(a);
+      k_yz_pipe<NN, N1_, false, C2><<<grid, kRegThreads, smem_yz_reg<NN, N1_, C2>(), h->stream>>>(a);
   });
   HE4_LAUNCHED(h);
   return HE4_OK;
@@ -724,11 +740,33 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
     HE4_REG_SWITCH(P.nz, P.n1[2], {
       constexpr int W = kRegThreads / N1_;
       a.map.W = W;
-      dim3 grid(nb, (unsigned)((total + W - 1) / W));
-      if (single)
-        k_zconv_reg<NN, N1_, true, C2><<<grid, kRegThreads, smem_zconv<NN, N1_, true, C2>(), h->stream>>>(a);
-      else
-        k_zconv_reg<NN, N1_, false, C2><<<grid, kRegThreads, smem_zconv<NN, N1_, false, C2>(), h->stream>>>(a);
+      const long ntiles = (total + W - 1) / W;
+      static int per_sm[2] = {0, 0};
+      int &ps = per_sm[single ? 1 : 0];
+      if (ps == 0) {
+        int dev = 0, nsm = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (single)
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zconv_pipe<NN, N1_, true, C2>, kRegThreads,
+                                                        smem_zpipe<NN, N1_, C2>());
+        else
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zconv_pipe<NN, N1_, false, C2>, kRegThreads,
+                                                        smem_zpipe<NN, N1_, C2>());
+        ps = std::max(1, occ) * std::max(1, nsm);
+      }
+      dim3 grid(nb, (unsigned)std::min<long>(ntiles, std::max(1, ps / nb)));
+      if (single) {
+        k_zconv_pipe<NN, N1_, true, C2><<<grid, kRegThreads, smem_zpipe<NN, N1_, C2>(), h->stream>>>(a);
+      } else if (sizeof(C2) == 16) {
+        k_zconv_pipe<NN, N1_, false, C2><<<grid, kRegThreads, smem_zpipe<NN, N1_, C2>(), h->stream>>>(a);
+      } else {
+        // FP32 with several outputs: the pipelined form's registers (two
+        // tiles, two kernel sets) leave one CTA per SM; the one-tile form
+        // with shared-memory kernel tiles is faster there
+        dim3 g1(nb, (unsigned)ntiles);
+        k_zconv_reg<NN, N1_, false, C2><<<g1, kRegThreads, smem_zconv<NN, N1_, false, C2>(), h->stream>>>(a);
+      }
     });
     HE4_LAUNCHED(h);
   }

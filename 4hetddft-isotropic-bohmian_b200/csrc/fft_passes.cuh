@@ -172,6 +172,56 @@ __global__ void __launch_bounds__(kRegThreads) k_yz_reg(YRegArgs<C2> a) {
     for (int k1 = 0; k1 < N1; k1++) data[off + ((j1 + N1 * c) + N2 * k1) * a.sf] = v[c * N1 + k1];
 }
 
+// Persistent, software-pipelined form of k_yz_reg: each CTA walks the
+// pencil tiles blockIdx.x, blockIdx.x + gridDim.x, ... and loads the next
+// tile's values into registers before transforming the current one, so the
+// next tile's loads are in flight during the current tile's FFT and stores.
+template <int N, int N1, bool INV, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_yz_pipe(YRegArgs<C2> a) {
+  constexpr int N2 = N / N1, W = kRegThreads / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
+  load_tw_n<N>(tw, a.tw);
+  __syncthreads();
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  C2 *data = a.buf[blockIdx.y];
+  const long ntiles = (a.map.nxh * (long)a.map.nother + W - 1) / W;
+  auto pencil = [&](long tile) -> long {
+    if (tile >= ntiles) return -1;
+    int kx, o;
+    long of = pencil_offset(a.map, tile * W + w, &kx, &o);
+    if (a.box && of >= 0) {
+      int lo, hi;
+      force_range(a.box, 2, a.nz, &lo, &hi);
+      if (o < lo || o > hi) of = -1;
+    }
+    return of;
+  };
+  long t = blockIdx.x;
+  long off = pencil(t);
+  C2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? data[off + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+  regfft::LayoutYZ lay{W, w};
+  for (; t < ntiles; t += gridDim.x) {
+    const long offn = pencil(t + gridDim.x);
+    C2 vn[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++)
+      vn[j2] = (offn >= 0) ? data[offn + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+    regfft::fwd2<N, N1, INV>(v, S, lay, j1, tw);
+    if (off >= 0) {
+#pragma unroll
+      for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) data[off + ((j1 + N1 * c) + N2 * k1) * a.sf] = v[c * N1 + k1];
+    }
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) v[j2] = vn[j2];
+    off = offn;
+  }
+}
+
 // z pass: one input per group, FFT_z once, then for each output
 // IFFT_z(coef * K(k) [* i D(k)] * X).  The kernel values K of an output are
 // copied to shared memory with cp.async one output ahead (the first ones
@@ -253,6 +303,105 @@ __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
       }
     }
   }
+}
+
+// Persistent, software-pipelined z pass: each CTA walks the pencil tiles of
+// one group; the next tile's input and the current output's kernel values
+// are loaded into registers ahead of the transforms that need them.
+template <int N, int N1, bool SINGLE, typename C2>
+__global__ void __launch_bounds__(kRegThreads) k_zconv_pipe(ZRegArgs<C2> a) {
+  using T = typename regfft::Re<C2>::type;
+  constexpr int N2 = N / N1, W = kRegThreads / N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
+  load_tw_n<N>(tw, a.tw);
+  __syncthreads();
+  const ZGroupT<C2> &G = a.g[blockIdx.x];
+  const int nout = SINGLE ? 1 : G.nout;
+  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
+  const long ntiles = (a.map.nxh * (long)a.map.nother + W - 1) / W;
+  auto pencil = [&](long tile, int *kx, int *ky) -> long {
+    *kx = 0;
+    *ky = 0;
+    if (tile >= ntiles) return -1;
+    return pencil_offset(a.map, tile * W + w, kx, ky);
+  };
+  auto load_k = [&](const T *kern, long off, T (&K)[N2]) {
+#pragma unroll
+    for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) {
+        const int k = (j1 + N1 * c) + N2 * k1;
+        K[c * N1 + k1] = (kern && off >= 0) ? __ldg(kern + off + (long)k * a.sf) : T(0);
+      }
+  };
+  regfft::LayoutYZ lay{W, w};
+  long t = blockIdx.y;
+  int kx, ky;
+  long off = pencil(t, &kx, &ky);
+  C2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? G.in[off + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+  for (; t < ntiles; t += gridDim.y) {
+    int kxn, kyn;
+    const long offn = pencil(t + gridDim.y, &kxn, &kyn);
+    C2 vn[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++)
+      vn[j2] = (offn >= 0) ? G.in[offn + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
+    T K[N2];
+    load_k(G.o[0].kern, off, K);
+    regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
+    const T dx = (off >= 0) ? a.dsym[kx] : T(0);
+    const T dy = (off >= 0) ? a.dsym[a.nx + ky] : T(0);
+    for (int o = 0; o < nout; o++) {
+      T Kn[SINGLE ? 1 : N2];
+      if (!SINGLE && o + 1 < nout) load_k(G.o[o + 1].kern, off, *reinterpret_cast<T(*)[N2]>(Kn));
+      const ZOutT<C2> Z = G.o[o];
+      C2 u[SINGLE ? 1 : N2];
+      C2 *x = SINGLE ? v : u;
+      const T coef = (T)Z.coef;
+#pragma unroll
+      for (int c = 0; c < N2 / N1; c++)
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) {
+          const int k = (j1 + N1 * c) + N2 * k1;
+          T cf = coef;
+          if (Z.kern && off >= 0) cf *= K[c * N1 + k1];
+          C2 y = regfft::scale(v[c * N1 + k1], cf);
+          if (Z.dsym_axis >= 0) {
+            const T ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
+            y = regfft::mk<C2>(-y.y * ds, y.x * ds);
+          }
+          x[c * N1 + k1] = y;
+        }
+      regfft::bwd2<N, N1, true>(*reinterpret_cast<C2(*)[N2]>(x), S, lay, j1, tw);
+      if (off >= 0) {
+        int zlo = 0, zhi = N - 1;
+        if (Z.boxz) force_range(a.box, 2, a.nz, &zlo, &zhi);
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) {
+          const int z = j1 + N1 * n2;
+          if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+        }
+      }
+      if (!SINGLE) {
+#pragma unroll
+        for (int e = 0; e < N2; e++) K[e] = Kn[SINGLE ? 0 : e];
+      }
+    }
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) v[j2] = vn[j2];
+    off = offn;
+    kx = kxn;
+    ky = kyn;
+  }
+}
+
+template <int N, int N1, typename C2>
+inline size_t smem_zpipe() {
+  constexpr int W = kRegThreads / N1;
+  return sizeof(C2) * ((size_t)N * W + N);
 }
 
 // x pass R2C: two real rows per complex pencil, Hermitian split
@@ -441,6 +590,14 @@ inline int reg_attrs() {
                                     (int)smem_yz_reg<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_yz_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_pipe<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_yz_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_pipe<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_yz_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_pipe<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zpipe<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_pipe<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_zpipe<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_zconv<N, N1, true, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
