@@ -554,6 +554,29 @@ def reference_arm(args):
     }), flush=True)
 
 
+def profile_kernels(form):
+    """One field evaluation of the 256^3 workload, then one warm-up and one
+    timed launch of each pass he4_bench_kernel measures: the workload the
+    ncu summaries under profiles/ capture (profiles/fft_passes_c3.md)."""
+    pkg = load_pkg()
+    w = pkg.workloads
+    p, psi, r, v, _ = w.workload("c3")
+    g = pkg.He4Step(form_params(pkg, p, form))
+    g.set_state(psi, r, v)
+    g.field()
+    L = pkg.load_library()
+    L.he4_bench_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), C.c_char_p, C.c_int32]
+    for which in (0, 1, 2, 3, 6, 7, 8):
+        ms, b = C.c_double(), C.c_double()
+        nm = C.create_string_buffer(64)
+        if L.he4_bench_kernel(g._h, which, 1, C.byref(ms), C.byref(b), nm, 64) != 0:
+            raise RuntimeError(L.he4_last_error().decode())
+        print(json.dumps({"which": which, "kernel": nm.value.decode(), "algorithmic_bytes": b.value,
+                          "ms": ms.value}), flush=True)
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -569,7 +592,12 @@ def main():
     ap.add_argument("--ensemble", type=int, default=64, help="ensemble members timed beside (0 = skip)")
     ap.add_argument("--ensemble-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-kernels", choices=["fp64", "fp32"], default=None,
+                    help="run each FFT/stencil pass once on the 256^3 workload (for ncu captures) and exit")
     args = ap.parse_args()
+    if args.profile_kernels:
+        profile_kernels(args.profile_kernels)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
