@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kRegThreads) k_yz_reg(YRegArgs<C2> a) {
 // tile's values into registers before transforming the current one, so the
 // next tile's loads are in flight during the current tile's FFT and stores.
 template <int N, int N1, bool INV, typename C2>
-__global__ void __launch_bounds__(kRegThreads) k_yz_pipe(YRegArgs<C2> a) {
+__global__ void __launch_bounds__(kRegThreads, sizeof(C2) == 8 ? 2 : 1) k_yz_pipe(YRegArgs<C2> a) {
   constexpr int N2 = N / N1, W = kRegThreads / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
@@ -309,7 +309,9 @@ __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
 // one group; the next tile's input and the current output's kernel values
 // are loaded into registers ahead of the transforms that need them.
 template <int N, int N1, bool SINGLE, typename C2>
-__global__ void __launch_bounds__(kRegThreads) k_zconv_pipe(ZRegArgs<C2> a) {
+// FP32: two CTAs per SM (128 registers) beat one CTA with no spills; FP64
+// spills heavily at that bound, so it keeps one CTA per SM
+__global__ void __launch_bounds__(kRegThreads, sizeof(C2) == 8 ? 2 : 1) k_zconv_pipe(ZRegArgs<C2> a) {
   using T = typename regfft::Re<C2>::type;
   constexpr int N2 = N / N1, W = kRegThreads / N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
