@@ -102,7 +102,7 @@ static void free_all(Handle *h) {
                   h->dyden, h->dzden, h->penalty, h->corr, h->denx, h->psix, h->hpsix, h->uimp, h->fx, h->fy,
                   h->fz, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], h->counts, h->rimp, h->vimp, h->aimp,
                   h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
-                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->box,
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->bub, h->box,
                   h->k32[0], h->k32[1], h->k32[2], h->k32[3], h->dsym32};
   for (void *p : ptrs) cudaFree(p);
   for (int i = 0; i < 8; i++) cudaFree(h->spec[i]);
@@ -476,6 +476,25 @@ int he4_diagnostics(he4_handle *hh, int32_t n4, double out[4]) {
     return HE4_E_ARG;
   }
   return compute_diagnostics(h, n4, out);
+}
+
+int he4_bubble_radius(he4_handle *hh, int32_t nr, double *rb, int32_t found[2], int32_t *ir, double xms[3],
+                      double *rr, double *denr) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  if (!rb || !found) {
+    set_error("he4_bubble_radius needs rb and found");
+    return HE4_E_ARG;
+  }
+  BubbleResult res;
+  HE4_TRY(compute_bubble_radius(h, nr, &res, rr, denr));
+  *rb = res.rb;
+  found[0] = res.found[0];
+  found[1] = res.found[1];
+  if (ir) *ir = res.ir;
+  if (xms)
+    for (int c = 0; c < 3; c++) xms[c] = res.xms[c];
+  return HE4_OK;
 }
 
 int he4_get_field(he4_handle *hh, int32_t which, double *out) {

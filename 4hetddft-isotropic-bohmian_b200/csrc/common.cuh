@@ -186,6 +186,9 @@ struct Handle {
   double *red = nullptr;      // partial sums workspace
   double *scal = nullptr;     // device scalars (errors, energies, means)
   double *hscal = nullptr;    // pinned host mirror of scal
+  // radial histogram of the spherical bubble radius (grown on demand)
+  unsigned long long *bub = nullptr;
+  size_t bub_len = 0;
 
   int have_state = 0;
   int nsteps_done = 0;
@@ -293,6 +296,17 @@ StepState get_step_state(const Handle *h, double dt);
 void set_step_state(Handle *h, const StepState &s);
 int compute_energy(Handle *h, he4_energies *e);
 int compute_diagnostics(Handle *h, int n4, double *host_out);
+// spherical bubble radius around the mean impurity position; rr / denr may
+// be null, otherwise they receive nr values
+struct BubbleResult {
+  double rb = 0.0;
+  double xms[3] = {0.0, 0.0, 0.0};
+  int found[2] = {0, 0};
+  int ir = 0;
+};
+int compute_bubble_radius(Handle *h, int nr, BubbleResult *res, double *rr, double *denr);
+int spline_global(const double *x, const double *y, double *A, double *B, double *C, double *D, double s1,
+                  double sn, int n);
 int compute_den(Handle *h);
 int particle_means(Handle *h, double *means);
 

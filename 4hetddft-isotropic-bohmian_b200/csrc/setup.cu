@@ -250,8 +250,8 @@ static double pair_pot(const he4_params &p, double r) {
 
 // cubic spline with end second derivatives s1, sn; global-form coefficients
 // a + x(b + x(c + x d)) per interval (Maron's algorithm, mates.f:36-117)
-static int spline_global(const double *x, const double *y, double *A, double *B, double *C, double *D, double s1,
-                         double sn, int n) {
+int spline_global(const double *x, const double *y, double *A, double *B, double *C, double *D, double s1,
+                  double sn, int n) {
   if (n < 4) return HE4_E_ARG;
   const int n1 = n - 1, n2 = n - 2;
   // 0-based: a[i] = h_i, d[i] = divided difference

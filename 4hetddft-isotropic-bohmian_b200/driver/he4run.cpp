@@ -90,6 +90,10 @@ struct Run {
   std::vector<double> vq;  // tabulated Vq (vqfile)
   int npar = 0, n4 = 300, niter = 0, iter0 = 0, pener = 50, pcurr = 0, icurr = 0;
   bool lrk = false, binary = false;
+  // spherical bubble radius of the pener block (DFT4He3d.f90:126-135,698-760)
+  bool lbubble = false, lspherical = true;
+  int nr = 501;
+  std::string file_spherical_bubble;
   double deltat = 0, deltatps = 0, time0 = 0;
   std::string filedenin, fileimpin, filedenout, fileimpout, filerimp, filevimp, fileaimp;
 };
@@ -161,6 +165,10 @@ void load_input(Run &r, const std::string &text) {
   r.icurr = (int)nl.integer("icurr", 0);
   r.time0 = nl.real("time0", 0.0);
   r.lrk = nl.logical("lrk", false);
+  r.lbubble = nl.logical("lbubble_radius", false);
+  r.lspherical = nl.logical("lspherical_bubble", true);
+  r.nr = (int)nl.integer("nr", 501);
+  r.file_spherical_bubble = nl.str("file_spherical_bubble", "spherical_bubble.out");
   // Delta t in K^-1 or ps (DFT4He3d.f90:229-243)
   r.deltat = nl.real("deltat", 0.0);
   r.deltatps = nl.real("deltatps", 0.0);
@@ -235,6 +243,24 @@ void denx_cuts(he4_handle *h, const Run &r, const double means[9]) {
   fclose(f);
 }
 
+// Lbubble_radius block (DFT4He3d.f90:929-986): the impurity mean-square
+// radii, then with Lspherical_bubble the spherical bubble radius, written
+// to file_spherical_bubble when both searches succeed.  The axial radii of
+// bubble_radius.f90 are not computed.
+void bubble_block(he4_handle *h, const Run &r, FILE *f62, double time) {
+  if (!r.lbubble) return;
+  double rb = 0.0, xms[3];
+  int32_t found[2] = {0, 0}, ir = 0;
+  check(he4_bubble_radius(h, r.nr, &rb, found, &ir, xms, nullptr, nullptr), "he4_bubble_radius");
+  printf(" Impurity mean square radius:(X),(Y),(Z): %s%s%s\n", fmt_e(xms[0], 15, 6).c_str(),
+         fmt_e(xms[1], 15, 6).c_str(), fmt_e(xms[2], 15, 6).c_str());
+  if (r.lspherical && found[0] && found[1]) {
+    printf("Spherical bubble radius........:%s\n", fmt_e(rb, 15, 6).c_str());
+    fprintf(f62, "%s%s\n", fmt_e(time, 15, 6).c_str(), fmt_e(rb, 18, 10).c_str());
+    fflush(f62);
+  }
+}
+
 int roundtrip(int argc, char **argv, bool binary) {
   if (argc < 4) die("--roundtrip needs psi_in imp_in psi_out imp_out");
   he4io::GridHeader g;
@@ -296,6 +322,11 @@ int main(int argc, char **argv) {
   FILE *f81 = fopen(r.filerimp.c_str(), "w"), *f82 = fopen(r.filevimp.c_str(), "w"),
        *f83 = fopen(r.fileaimp.c_str(), "w");
   if (!f81 || !f82 || !f83) die("cannot open the trajectory files");
+  FILE *f62 = nullptr;
+  if (r.lbubble && r.lspherical) {
+    f62 = fopen(r.file_spherical_bubble.c_str(), "w");
+    if (!f62) die("cannot open file_spherical_bubble");
+  }
   // first field and energy (DFT4He3d.f90:630-660)
   check(he4_field(h), "he4_field");
   double diag[4];
@@ -318,6 +349,7 @@ int main(int argc, char **argv) {
   he4_energies e;
   check(he4_energy(h, &e), "he4_energy");
   printf("Number of He4 atoms%s\n", fmt_e(diag[0], 15, 6).c_str());
+  bubble_block(h, r, f62, r.time0);
   double eold = e.etot;
   // the time loop (DFT4He3d.f90:848-1045)
   const int first = r.iter0 + 1;
@@ -350,6 +382,7 @@ int main(int argc, char **argv) {
       printf("C.M. V..:%s%s%s\n", fmt_e(means[3], 15, 6).c_str(), fmt_e(means[4], 15, 6).c_str(),
              fmt_e(means[5], 15, 6).c_str());
       denx_cuts(h, r, means);
+      bubble_block(h, r, f62, time);
       fflush(stdout);
     }
     if (r.pcurr > 0 && iter % r.pcurr == 0) {
@@ -361,6 +394,7 @@ int main(int argc, char **argv) {
   fclose(f81);
   fclose(f82);
   fclose(f83);
+  if (f62) fclose(f62);
   printoutc(h, r, time, 1, r.filedenout, r.fileimpout, iter);
   he4_destroy(h);
   return 0;

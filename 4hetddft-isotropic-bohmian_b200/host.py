@@ -51,6 +51,7 @@ def load_library():
     L.he4_energy.argtypes = [vp, vp]
     L.he4_get_field.argtypes = [vp, i32, dp]
     L.he4_diagnostics.argtypes = [vp, i32, dp]
+    L.he4_bubble_radius.argtypes = [vp, i32, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), dp, dp, dp]
     L.he4_get_kernel.argtypes = [vp, i32, dp]
     L.he4_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.he4_device_ptr.argtypes = [vp, i32, C.POINTER(vp)]
@@ -221,6 +222,20 @@ class He4Step:
         out = np.zeros(4)
         _check(load_library().he4_diagnostics(self._h, n4, _dp(out)), "he4_diagnostics")
         return out
+
+    def bubble_radius(self, nr=501):
+        """Spherical bubble radius of the current state (Bubble_Radius_esferic,
+        bubble_radius_esferic.f90:1-134, with the caller's ipx and xmsx of
+        DFT4He3d.f90:893-947).  Returns a dict with rb, lcontrol (two bools),
+        ir (1-based bin of the density maximum), xms (3), rr and denr (nr)."""
+        rb = C.c_double(0.0)
+        found = (C.c_int32 * 2)()
+        ir = C.c_int32(0)
+        xms, rr, denr = np.zeros(3), np.zeros(nr), np.zeros(nr)
+        _check(load_library().he4_bubble_radius(self._h, nr, C.byref(rb), found, C.byref(ir), _dp(xms), _dp(rr),
+                                                _dp(denr)), "he4_bubble_radius")
+        return {"rb": rb.value, "lcontrol": (bool(found[0]), bool(found[1])), "ir": ir.value, "xms": xms,
+                "rr": rr, "denr": denr}
 
     def get_field(self, name):
         out = np.zeros(self.shape)

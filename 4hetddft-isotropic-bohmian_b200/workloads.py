@@ -84,6 +84,21 @@ def droplet_psi(p, n4):
     return np.sqrt(rho).astype(np.complex128)
 
 
+def bubble_psi(p, n4, center, rb, wall=0.5, bump=0.3):
+    """Droplet psi with a spherical cavity of radius rb around `center`:
+    rho = drop(r) * g(|r - center|), g rising through 1/2 at rb over `wall`
+    A with a `bump` overshoot (the density shell that forms around a
+    solvated impurity).  complex128 array [nz][ny][nx]."""
+    x, y, z = grid_axes(p)
+    rr = np.sqrt(z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2)
+    R = 2.22 * n4 ** (1.0 / 3.0)
+    rho = RHO0 / (1.0 + np.exp((rr - R) / AFERMI))
+    c = np.asarray(center, dtype=np.float64)
+    s = np.sqrt((z[:, None, None] - c[2]) ** 2 + (y[None, :, None] - c[1]) ** 2 + (x[None, None, :] - c[0]) ** 2)
+    g = (1.0 + bump * np.exp(-((s - rb - 4.0 * wall) / (2.0 * wall)) ** 2)) / (1.0 + np.exp(-(s - rb) / wall))
+    return np.sqrt(rho * g).astype(np.complex128)
+
+
 def particles(npar, seed, speed_ms, center=(0.0, 0.0, 2.0), width=0.3):
     """Test particles from an isotropic Gaussian of the given width around
     `center`, all moving toward the droplet centre (the origin) at speed_ms.

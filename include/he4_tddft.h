@@ -159,6 +159,24 @@ int he4_energy(he4_handle *h, he4_energies *e);
  * of den (r_cm.f90:23-58, divided by n4 as r_cm does). */
 int he4_diagnostics(he4_handle *h, int32_t n4, double out[4]);
 
+/* Spherical bubble radius around the impurity, the Lspherical_bubble
+ * diagnostic of the pener block (DFT4He3d.f90:929-986 with
+ * bubble_radius_esferic.f90:1-134), reduced on the device.  The centre is
+ * the grid point (ipx,ipy,ipz) of the mean trajectory position
+ * (DFT4He3d.f90:893-898); xms[3] receives the impurity mean-square radii
+ * sqrt(sum denx x^2 dxyz) (DFT4He3d.f90:933-947).  den is averaged over nr
+ * radial bins of width dr = rmax/(nr-1) (the reference uses nr = 501),
+ * normalised to the atom number and splined; found[0] reports the first
+ * density maximum past max(xms) (Lcontrol(1)), found[1] the half-maximum
+ * crossing refined by Newton iterations (Lcontrol(2)); rb is the radius
+ * when both are set; ir the 1-based bin of the maximum (0 if none).  rr and
+ * denr (nr values each, may be NULL) receive the radii and the normalised
+ * radial density.  The reference stops when a grid point lies past rmax
+ * (the mean position has a positive grid coordinate); this returns
+ * HE4_E_ARG instead.  nr must lie in [4, 8192]. */
+int he4_bubble_radius(he4_handle *h, int32_t nr, double *rb, int32_t found[2],
+                      int32_t *ir, double xms[3], double *rr, double *denr);
+
 /* he4_diagnostics without a handle and without any allocation.  It has no
  * counterpart in the reference; it exists for callers that cannot call
  * cudaMalloc: hosts whose device memory belongs to another allocator (a

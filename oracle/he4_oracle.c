@@ -1560,6 +1560,185 @@ int ora_diagnostics(ora_state *s, int32_t n4, double out[4]) {
   return HE4_OK;
 }
 
+/* Spherical bubble radius: the Lspherical_bubble block of the pener
+ * diagnostics (DFT4He3d.f90:893-898 ipx/ipy/ipz, :933-947 xmsx/ymsx/zmsx)
+ * and Bubble_Radius_esferic (bubble_radius_esferic.f90:1-134), sequential
+ * loops in the reference's order.  Arrays are 1-based views as in the
+ * Fortran.  Where the reference stops ('0001', a point past rmax) this
+ * returns HE4_E_ARG. */
+int ora_bubble_search(int32_t nr, double dr, double xnorm, const double xms[3], double *rr0, double *denr0,
+                      double *rb_out, int32_t found[2], int32_t *ir_out) {
+  if (nr < 4 || !rr0 || !denr0 || !rb_out || !found) return HE4_E_ARG;
+  double *rr = rr0 - 1, *denr = denr0 - 1;
+  double *work = malloc(sizeof(double) * 4 * (size_t)nr);
+  if (!work) return HE4_E_NOMEM;
+  double *A = work - 1, *B = A + nr, *C = B + nr, *D = C + nr;
+  /* denmin = MaxVal(denr)*0.75 before the normalisation (:66) */
+  double dmax = denr[1];
+  for (int i = 2; i <= nr; i++)
+    if (denr[i] > dmax) dmax = denr[i];
+  double denmin = dmax * 0.75;
+  double aux1 = 0.0;
+  for (int i = 1; i <= nr; i++) { /* :68-74 */
+    double r = (double)(i - 1) * dr;
+    rr[i] = r;
+    double r2 = r * r;
+    aux1 = aux1 + r2 * denr[i];
+  }
+  aux1 = aux1 * dr * 4.0 * PI;
+  double fac = xnorm / aux1;
+  for (int i = 1; i <= nr; i++) denr[i] = denr[i] * fac;
+  found[0] = found[1] = 0;
+  *rb_out = 0.0;
+  if (ir_out) *ir_out = 0;
+  int e = ora_spline(rr + 1, denr + 1, A + 1, B + 1, C + 1, D + 1, 0.0, 0.0, nr); /* :77 */
+  if (e) {
+    free(work);
+    return HE4_OK;
+  }
+  double r_min = 2.0;
+  double am = xms[0];
+  if (xms[1] > am) am = xms[1];
+  if (xms[2] > am) am = xms[2];
+  int i = (int)(am / dr + 1.5);
+  int ir = 0, j;
+  /* :80-86; j = 1 would read denr(0), so the scan starts at 2 */
+  for (j = (i < 2 ? 2 : i); j <= nr - 1; j++) {
+    if (denr[j] > denr[j - 1] && denr[j] > denr[j + 1]) {
+      if (rr[j] < r_min || denr[j] < denmin) continue;
+      ir = j;
+      found[0] = 1;
+      break;
+    }
+  }
+  if (j == nr - 1 || j > nr - 1) { /* :87 */
+    found[0] = 0;
+    free(work);
+    return HE4_OK;
+  }
+  if (ir_out) *ir_out = ir;
+  double aux2 = denr[ir] * 0.5; /* :100 */
+  int it = (int)(am / dr + 1.5);
+  for (j = ir - 1; j >= it + 1; j--) { /* :102-108 */
+    if ((denr[j - 1] - aux2) * (denr[j + 1] - aux2) < 0.0) {
+      i = j;
+      found[1] = 1;
+      break;
+    }
+  }
+  if (j == it || j == it - 1) { /* :110 */
+    found[1] = 0;
+    free(work);
+    return HE4_OK;
+  }
+  double rb = rr[i];
+  const int niter = 100;
+  const double eps = 1.0e-6;
+  for (it = 1; it <= niter; it++) { /* :117-125 */
+    double f = ((D[i] * rb + C[i]) * rb + B[i]) * rb + A[i];
+    double df = (3.0 * D[i] * rb + 2.0 * C[i]) * rb + B[i];
+    double step = -(f - aux2) / df;
+    rb = rb + step;
+    if (fabs(step) < eps) break;
+  }
+  *rb_out = rb;
+  if (it == niter || it == niter + 1) found[1] = 0; /* :126 */
+  free(work);
+  return HE4_OK;
+}
+
+int ora_bubble_radius(ora_state *s, int32_t nr, double *rb, int32_t found[2], int32_t *ir, double xms[3],
+                      double *rr, double *denr) {
+  if (!s || !rb || !found || nr < 4 || nr > 8192) return HE4_E_ARG;
+  if (!s->have_state) return HE4_E_STATE;
+  if (!s->field_valid) {
+    int e0 = ora_field(s);
+    if (e0) return e0;
+  }
+  const he4_params *p = &s->p;
+  int nx = s->nx, ny = s->ny, nz = s->nz, np = p->n_par;
+  /* mean trajectory position and its grid point (DFT4He3d.f90:893-898) */
+  double mean[3];
+  for (int c = 0; c < 3; c++) {
+    double a = 0.0;
+    for (int k = 0; k < np; k++) a += s->rimp[(size_t)c * np + k];
+    mean[c] = a / np;
+  }
+  const double xmx[3] = {p->xmax, p->ymax, p->zmax}, hh[3] = {s->hx, s->hy, s->hz};
+  const int nn[3] = {nx, ny, nz};
+  int ip[3];
+  for (int c = 0; c < 3; c++) {
+    double t = 1.5 + (mean[c] + xmx[c]) / hh[c];
+    if (!(t >= 1.0 && t < nn[c] + 1.0)) return HE4_E_ARG;
+    ip[c] = (int)t; /* 1-based */
+  }
+  /* xmsx, ymsx, zmsx (:933-947) */
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int iz = 0; iz < nz; iz++)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++) {
+        double w = s->denx[((size_t)iz * ny + iy) * nx + ix];
+        sx = sx + w * (s->x[ix] * s->x[ix]);
+        sy = sy + w * (s->y[iy] * s->y[iy]);
+        sz = sz + w * (s->z[iz] * s->z[iz]);
+      }
+  double ms[3] = {sqrt(sx * s->dxyz), sqrt(sy * s->dxyz), sqrt(sz * s->dxyz)};
+  if (xms)
+    for (int c = 0; c < 3; c++) xms[c] = ms[c];
+  /* Bubble_Radius_esferic (:19-31) */
+  double *X = s->x - 1, *Y = s->y - 1, *Z = s->z - 1; /* 1-based */
+  double hx = X[2] - X[1], hy = Y[2] - Y[1], hz = Z[2] - Z[1];
+  double ex = -X[1] - X[ip[0]], ey = -Y[1] - Y[ip[1]], ez = -Z[1] - Z[ip[2]];
+  double rmax = sqrt(ex * ex + ey * ey + ez * ez);
+  double dr = rmax / (nr - 1);
+  double dxyz = hx * hy * hz;
+  double sden = 0.0;
+  for (size_t t = 0; t < s->N; t++) sden += s->den[t];
+  double xnorm = sden * dxyz;
+  double *dr_ = calloc((size_t)nr, sizeof(double)), *rr_ = malloc(sizeof(double) * nr);
+  long long *norm = calloc((size_t)nr, sizeof(long long));
+  if (!dr_ || !rr_ || !norm) {
+    free(dr_);
+    free(rr_);
+    free(norm);
+    return HE4_E_NOMEM;
+  }
+  int bad = 0;
+  for (int iz = 1; iz <= nz && !bad; iz++) { /* :45-62 */
+    double z2 = (Z[iz] - Z[ip[2]]) * (Z[iz] - Z[ip[2]]);
+    for (int iy = 1; iy <= ny && !bad; iy++) {
+      double y2 = (Y[iy] - Y[ip[1]]) * (Y[iy] - Y[ip[1]]);
+      for (int ix = 1; ix <= nx; ix++) {
+        double x2 = (X[ix] - X[ip[0]]) * (X[ix] - X[ip[0]]);
+        double r = sqrt(x2 + y2 + z2);
+        double t = r / dr + 1.5;
+        if (!(t < nr + 1.0)) { /* ir > nr: Stop '0001' */
+          bad = 1;
+          break;
+        }
+        int b = (int)t;
+        dr_[b - 1] += s->den[(((size_t)iz - 1) * ny + (iy - 1)) * nx + (ix - 1)];
+        norm[b - 1] += 1;
+      }
+    }
+  }
+  if (bad) {
+    free(dr_);
+    free(rr_);
+    free(norm);
+    return HE4_E_ARG;
+  }
+  for (int b = 0; b < nr; b++)
+    if (norm[b] != 0) dr_[b] = dr_[b] / (double)norm[b];
+  int e = ora_bubble_search(nr, dr, xnorm, ms, rr_, dr_, rb, found, ir);
+  if (rr) memcpy(rr, rr_, sizeof(double) * nr);
+  if (denr) memcpy(denr, dr_, sizeof(double) * nr);
+  free(dr_);
+  free(rr_);
+  free(norm);
+  return e;
+}
+
 int ora_get_field(ora_state *s, int32_t which, double *out) {
   if (!s || !out) return HE4_E_ARG;
   const double *src = NULL;

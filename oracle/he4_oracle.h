@@ -36,6 +36,8 @@ int ora_run(ora_state *s, int32_t nsteps, double deltat, double *err,
             double *means);
 int ora_energy(ora_state *s, he4_energies *e);
 int ora_diagnostics(ora_state *s, int32_t n4, double out[4]);
+int ora_bubble_radius(ora_state *s, int32_t nr, double *rb, int32_t found[2],
+                      int32_t *ir, double xms[3], double *rr, double *denr);
 int ora_get_field(ora_state *s, int32_t which, double *out);
 int ora_get_kernel(ora_state *s, int32_t which, double *out);
 void ora_set_threads(int n);
@@ -48,6 +50,11 @@ int ora_fft3_c2r(int nx, int ny, int nz, const double *in, double *out);
 int ora_spline(const double *x, const double *y, double *a, double *b,
                double *c, double *d, double s1, double sn, int n);
 int ora_deriv(ora_state *s, int id, int axis, const double *f, double *df);
+/* The search half of Bubble_Radius_esferic on a binned radial density
+ * (denr is normalised in place; rr receives the bin radii). */
+int ora_bubble_search(int32_t nr, double dr, double xnorm, const double xms[3],
+                      double *rr, double *denr, double *rb, int32_t found[2],
+                      int32_t *ir);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,9 @@ def _declare(L):
     L.ora_run.argtypes = [vp, i32, C.c_double, dp, dp]
     L.ora_energy.argtypes = [vp, vp]
     L.ora_diagnostics.argtypes = [vp, i32, dp]
+    ip = C.POINTER(C.c_int32)
+    L.ora_bubble_radius.argtypes = [vp, i32, dp, ip, ip, dp, dp, dp]
+    L.ora_bubble_search.argtypes = [i32, C.c_double, C.c_double, dp, dp, dp, dp, ip, ip]
     L.ora_get_field.argtypes = [vp, i32, dp]
     L.ora_get_kernel.argtypes = [vp, i32, dp]
     L.ora_set_threads.argtypes = [C.c_int]
@@ -192,6 +195,16 @@ class Oracle:
         _check(lib().ora_diagnostics(self._h, n4, _dp(out)), "diagnostics")
         return out
 
+    def bubble_radius(self, nr=501):
+        rb = C.c_double(0.0)
+        found = (C.c_int32 * 2)()
+        ir = C.c_int32(0)
+        xms, rr, denr = np.zeros(3), np.zeros(nr), np.zeros(nr)
+        _check(lib().ora_bubble_radius(self._h, nr, C.byref(rb), found, C.byref(ir), _dp(xms), _dp(rr), _dp(denr)),
+               "bubble_radius")
+        return {"rb": rb.value, "lcontrol": (bool(found[0]), bool(found[1])), "ir": ir.value, "xms": xms,
+                "rr": rr, "denr": denr}
+
     def get_field(self, name):
         import sys
         ids = sys.modules["he4b200"].abi.FIELD_ID
@@ -211,3 +224,19 @@ class Oracle:
         out = np.zeros_like(f)
         _check(lib().ora_deriv(self._h, order, axis, _dp(f), _dp(out)), "deriv")
         return out
+
+
+def bubble_search(denr, dr, xnorm, xms):
+    """The search half of Bubble_Radius_esferic on a binned radial density
+    (bubble_radius_esferic.f90:63-132).  Returns (rb, (Lcontrol1, Lcontrol2),
+    ir, rr, normalised denr)."""
+    d = np.ascontiguousarray(denr, dtype=np.float64).copy()
+    nr = d.size
+    rr = np.zeros(nr)
+    x = np.ascontiguousarray(xms, dtype=np.float64)
+    rb = C.c_double(0.0)
+    found = (C.c_int32 * 2)()
+    ir = C.c_int32(0)
+    _check(lib().ora_bubble_search(nr, dr, xnorm, _dp(x), _dp(rr), _dp(d), C.byref(rb), found, C.byref(ir)),
+           "bubble_search")
+    return rb.value, (bool(found[0]), bool(found[1])), ir.value, rr, d

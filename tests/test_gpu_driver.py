@@ -71,3 +71,47 @@ def test_driver_run_matches_library(pkg, tmp_path):
     assert np.array_equal(got, want)
     last_tot = [l for l in out.splitlines() if "TOTAL energy" in l][-1]
     assert float(last_tot.split()[-2]) == pytest.approx(e["etot"], abs=2e-6)
+
+
+def test_driver_spherical_bubble(pkg, tmp_path):
+    """Lbubble_radius: the driver writes the spherical bubble radius at the
+    start and every pener steps (DFT4He3d.f90:698-760,929-986); the values
+    equal he4_bubble_radius after the same call sequence."""
+    w = pkg.workloads
+    p = w.make_params(64, 0.6, 256)
+    center = (-0.5, -0.7, -2.0)
+    psi = w.bubble_psi(p, 300, center, 4.0)
+    r, v = w.particles(256, 7, 100.0, center=center)
+    d = str(tmp_path)
+    write_inputs(d, p, psi, r, v)
+    nml = f""" &input nx={p.nx}, ny={p.ny}, nz={p.nz}, xmax={p.xmax!r}, ymax={p.ymax!r}, zmax={p.zmax!r},
+   n4=300, mode=2, core4='OTC', npd=7, icon=8, N_par={p.n_par}, mimpur={p.mimpur!r},
+   deltatps=1.d-3, niter=6, pener=3, pcurr=0, ironx=1, lbubble_radius=.true., nr=97,
+   selec_gs='morse', morse_d={w.MORSE_D}, morse_alpha={w.MORSE_ALPHA}, morse_re={w.MORSE_RE},
+   r_cutoff_gs={p.r_cutoff!r}, umax_gs={p.umax!r}, nq={p.nq} /
+"""
+    res = subprocess.run([os.path.join(PKG, "he4run")], input=nml, capture_output=True, text=True, cwd=d)
+    assert res.returncode == 0, res.stderr[-2000:]
+    assert res.stdout.count("Impurity mean square radius") == 3
+    lines = open(os.path.join(d, "spherical_bubble.out")).read().splitlines()
+    dt = w.deltat_fs(1.0)
+    want = []
+    with pkg.He4Step(p) as g:
+        g.set_state(psi, r, v)
+        g.field()
+        g.energy()
+        want.append((0.0, g.bubble_radius(97)))
+        for it in range(1, 7):
+            if it <= 3:
+                g.steprk(dt)
+            else:
+                g.steppc(dt)
+            if it % 3 == 0:
+                g.energy()
+                want.append((it * 1e-3, g.bubble_radius(97)))
+    want = [(t, b["rb"]) for t, b in want if all(b["lcontrol"])]
+    assert len(want) >= 2 and len(lines) == len(want)
+    for l, (t, rb) in zip(lines, want):
+        tt, rr = map(float, l.split())
+        assert tt == pytest.approx(t, abs=1e-9)
+        assert rr == pytest.approx(rb, rel=1e-9)
