@@ -507,7 +507,7 @@ int he4_get_field(he4_handle *hh, int32_t which, double *out) {
   // fields a merged (time-step) evaluation leaves unwritten
   if (h->field_valid && !h->split_valid &&
       (which == HE4_F_UIMP || which == HE4_F_DELJ4 || which == HE4_F_UALPHAS || which == HE4_F_PENALTY ||
-       which == HE4_F_CORR))
+       which == HE4_F_CORR || which == HE4_F_FALFS))
     HE4_TRY(field_split_fields(h));
   switch (which) {
     case HE4_F_DEN: src = h->den; break;

@@ -208,6 +208,16 @@ struct Handle {
 
 // kernel-level entry points used by the ABI layer
 int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out);
+// x pass R2C whose input rows are formed on load from other grids:
+//   XLOAD_ALFA: in_f * (1 - aux0 * c0)     (falfs * d_f rho, term_alfa.f90:28-36)
+//   XLOAD_CORR: aux0 * aux1 * (c0 + c1 * aux1)  (poten.f90:62-64; `in` unused)
+enum { XLOAD_PLAIN = 0, XLOAD_ALFA = 1, XLOAD_CORR = 2 };
+struct XLoad {
+  int op = XLOAD_PLAIN;
+  const double *aux0 = nullptr, *aux1 = nullptr;
+  double c0 = 0.0, c1 = 0.0;
+};
+int fft_r2c_load(Handle *h, int n, const double *const *in, double2 *const *out, const XLoad &ld);
 int fft_c2r(Handle *h, int n, double2 *const *in, double *const *out);
 int fft_y(Handle *h, int n, double2 *const *buf, bool inverse);
 // z pass: for each op, out = IFFT_z(coef * K * FFT_z(in)); K may be null (=1)

@@ -486,7 +486,7 @@ void fft_plan_free(FftPlan &P) {
 // register-path x pass in the spectrum type C2 (the real grids stay FP64)
 template <typename C2>
 static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *const *cout, double2 *const *cin,
-                      double *const *rout, bool inverse, const BoxPair *box) {
+                      double *const *rout, bool inverse, const BoxPair *box, const XLoad &ld) {
   const FftPlan &P = h->fft;
   const long nrow = (long)P.ny * P.nz;
   XRegArgs<C2> a{};
@@ -497,6 +497,7 @@ static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *cons
   a.box = inverse ? box : nullptr;
   a.ny = P.ny;
   a.nz = P.nz;
+  a.ld = ld;
   for (int i = 0; i < nb; i++) {
     if (inverse) {
       a.cin[i] = reinterpret_cast<const C2 *>(cin[i]);
@@ -511,6 +512,10 @@ static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *cons
     dim3 grid((unsigned)((nrow + 2 * Pp - 1) / (2 * Pp)), nb);
     if (inverse)
       k_xc2r_reg<NN, N1_, C2><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
+    else if (ld.op == XLOAD_ALFA)
+      k_xr2c_reg<NN, N1_, C2, XLOAD_ALFA><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
+    else if (ld.op == XLOAD_CORR)
+      k_xr2c_reg<NN, N1_, C2, XLOAD_CORR><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
     else
       k_xr2c_reg<NN, N1_, C2><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
   });
@@ -520,7 +525,7 @@ static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *cons
 
 // box (C2R only, register path): restrict to the rows of the force box
 static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *cout, double2 *const *cin,
-                  double *const *rout, bool inverse, const BoxPair *box = nullptr) {
+                  double *const *rout, bool inverse, const BoxPair *box = nullptr, const XLoad &ld = XLoad()) {
   const FftPlan &P = h->fft;
   const long nrow = (long)P.ny * P.nz;
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
@@ -531,10 +536,14 @@ static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *co
       double2 *const *ci = cin ? cin + b0 : nullptr;
       double *const *ro = rout ? rout + b0 : nullptr;
       if (h->fp32)
-        HE4_TRY(x_pass_reg<float2>(h, nb, ri, co, ci, ro, inverse, box));
+        HE4_TRY(x_pass_reg<float2>(h, nb, ri, co, ci, ro, inverse, box, ld));
       else
-        HE4_TRY(x_pass_reg<double2>(h, nb, ri, co, ci, ro, inverse, box));
+        HE4_TRY(x_pass_reg<double2>(h, nb, ri, co, ci, ro, inverse, box, ld));
       continue;
+    }
+    if (ld.op != XLOAD_PLAIN) {
+      set_error("formed-on-load x pass needs a register-path axis length");
+      return HE4_E_UNSUPPORTED;
     }
     if (h->fp32) {
       set_error("FP32 spectra need register-path axis lengths");
@@ -663,6 +672,12 @@ int fft_y(Handle *h, int n, double2 *const *buf, bool inverse) { return strided_
 
 int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out) {
   HE4_TRY(x_pass(h, n, in, out, nullptr, nullptr, false));
+  HE4_TRY(fft_y(h, n, out, false));
+  return HE4_OK;
+}
+
+int fft_r2c_load(Handle *h, int n, const double *const *in, double2 *const *out, const XLoad &ld) {
+  HE4_TRY(x_pass(h, n, in, out, nullptr, nullptr, false, nullptr, ld));
   HE4_TRY(fft_y(h, n, out, false));
   return HE4_OK;
 }

@@ -108,7 +108,19 @@ struct XRegArgs {
   C2 *cout[kRegBatch];
   const C2 *cin[kRegBatch];
   double *rout[kRegBatch];
+  XLoad ld;  // R2C: how input rows are formed
 };
+
+// one input element of the R2C pass (XLoad; OP is the compile-time op)
+template <int OP>
+__device__ __forceinline__ double xload(const XLoad &ld, const double *__restrict__ in, long i) {
+  if (OP == XLOAD_ALFA) return (1.0 - ld.aux0[i] * ld.c0) * in[i];
+  if (OP == XLOAD_CORR) {
+    const double d = ld.aux0[i], c = ld.aux1[i];
+    return d * c * (ld.c0 + ld.c1 * c);
+  }
+  return in[i];
+}
 
 template <int N, typename C2>
 __device__ __forceinline__ void load_tw_n(C2 *s_tw, const C2 *__restrict__ g_tw) {
@@ -407,7 +419,7 @@ inline size_t smem_zpipe() {
 }
 
 // x pass R2C: two real rows per complex pencil, Hermitian split
-template <int N, int N1, typename C2>
+template <int N, int N1, typename C2, int OP = XLOAD_PLAIN>
 __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
   using T = typename regfft::Re<C2>::type;
   constexpr int N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
@@ -419,12 +431,20 @@ __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
   const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
   const double *in = a.rin[blockIdx.y];
   C2 *out = a.cout[blockIdx.y];
-  C2 v[N2];
+  // loads from clamped rows (unconditional, so they issue together), rows
+  // past the end zeroed afterwards
+  const long rac = ra < a.nrow ? ra : a.nrow - 1, rbc = rb < a.nrow ? rb : a.nrow - 1;
+  double xa[N2], xb[N2];
 #pragma unroll
   for (int j2 = 0; j2 < N2; j2++) {
     const int x = j1 + N1 * j2;
-    v[j2] = regfft::mk<C2>((T)((ra < a.nrow) ? in[ra * N + x] : 0.0), (T)((rb < a.nrow) ? in[rb * N + x] : 0.0));
+    xa[j2] = xload<OP>(a.ld, in, rac * N + x);
+    xb[j2] = xload<OP>(a.ld, in, rbc * N + x);
   }
+  C2 v[N2];
+#pragma unroll
+  for (int j2 = 0; j2 < N2; j2++)
+    v[j2] = regfft::mk<C2>((T)((ra < a.nrow) ? xa[j2] : 0.0), (T)((rb < a.nrow) ? xb[j2] : 0.0));
   regfft::LayoutX lay{p * SP};
   regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
   C2 *Sp = S + p * SP;
@@ -605,6 +625,10 @@ inline int reg_attrs() {
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_zconv<N, N1, false, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_x_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2, XLOAD_ALFA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_x_reg<N, N1, C2>()));
+  HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2, XLOAD_CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_x_reg<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_x_reg<N, N1, C2>()));

@@ -217,6 +217,22 @@ __global__ void k_alfa2(const double *__restrict__ dx, const double *__restrict_
   h2[t] = f * iz[t];
 }
 
+// k_alfa2 with falfs formed from denalf (merged evaluation, which does not
+// store falfs): f = 1 - denalf * (1/den0s)
+__global__ void k_alfa2m(const double *__restrict__ dx, const double *__restrict__ dy, const double *__restrict__ dz,
+                         const double *__restrict__ ix, const double *__restrict__ iy, const double *__restrict__ iz,
+                         const double *__restrict__ denalf, double inv_den0s, double *s, double *h0, double *h1,
+                         double *h2, size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double a = ix[t], b = iy[t], c = iz[t];
+  s[t] = (dx[t] * a) + (dy[t] * b) + (dz[t] * c);
+  const double f = 1.0 - denalf[t] * inv_den0s;
+  h0[t] = f * a;
+  h1[t] = f * b;
+  h2[t] = f * c;
+}
+
 // ualphas = (u1/den0s + sum_i d_i h_i) * h2o2m4 * alphas ; pot4 += ualphas
 // (term_alfa.f90:110-113, poten.f90:101-104)
 __global__ void k_alfa3(double *ualphas, const double *__restrict__ h0, const double *__restrict__ h1,
@@ -399,8 +415,10 @@ int field_potenimp(Handle *h, bool split) {
 
 // Merged form of poten (the time-step path): the linear convolutions that
 // enter pot4 (delj4, uimp, the correlation term and the alpha_s u1 term) are
-// summed in k space and inverted once; the named intermediate fields delj4,
-// uimp, corr, ualphas and penalty are not written.
+// summed in k space and inverted once; the correlation source and the
+// falfs*grad(rho) sources of term_alfa are formed inside the x pass that
+// transforms them; the named intermediate fields delj4, uimp, corr, ualphas,
+// penalty and falfs are not written.
 static int field_poten_merged(Handle *h) {
   const Geo g = geo(h);
   const size_t N = h->N;
@@ -420,24 +438,32 @@ static int field_poten_merged(Handle *h) {
     HE4_TRY(fft_c2r(h, otc ? 2 : 1, sp, out));
   }
   HE4_TRY(launch_grad(h));
-  // correlation source, x/y transform kept in spec[5]
-  k_corr_src<<<nblk(N), 256, 0, h->stream>>>(h->den, h->dencg, h->rtmp[0], N, ot);
-  HE4_LAUNCHED(h);
+  // correlation source den*dencg*(cp4+cpp4*dencg) formed in the x pass,
+  // x/y transform kept in spec[5]
   {
-    const double *in[1] = {h->rtmp[0]};
+    const double *in[1] = {h->den};
     double2 *sp[1] = {h->spec[5]};
-    HE4_TRY(fft_r2c(h, 1, in, sp));
+    XLoad ld;
+    ld.op = XLOAD_CORR;
+    ld.aux0 = h->den;
+    ld.aux1 = h->dencg;
+    ld.c0 = ot.cp4;
+    ld.c1 = ot.cpp4;
+    HE4_TRY(fft_r2c_load(h, 1, in, sp, ld));
   }
   ZTerm terms[4] = {{h->spec[0], h->fvlj4, h->renor}, {h->spec[4], h->vq, h->renor}, {h->spec[5], h->wcgk, h->renor},
                     {h->spec[1], h->kalfs, h->renor * h->p.h2o2m4 * h->p.alphas / h->p.den0s}};
   if (otc) {
-    k_alfa1<<<nblk(N), 256, 0, h->stream>>>(h->denalf, h->dxden, h->dyden, h->dzden, h->falfs, h->rtmp[0],
-                                           h->rtmp[1], h->rtmp[2], N, ot);
-    HE4_LAUNCHED(h);
+    const double inv_den0s = 1.0 / h->p.den0s;
     {
-      const double *in[3] = {h->rtmp[0], h->rtmp[1], h->rtmp[2]};
+      // g_i = falfs * d_i rho formed in the x pass (falfs is not stored)
+      const double *in[3] = {h->dxden, h->dyden, h->dzden};
       double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
-      HE4_TRY(fft_r2c(h, 3, in, sp));
+      XLoad ld;
+      ld.op = XLOAD_ALFA;
+      ld.aux0 = h->denalf;
+      ld.c0 = inv_den0s;
+      HE4_TRY(fft_r2c_load(h, 3, in, sp, ld));
       ZOp ops[3] = {{h->spec[1], h->spec[1], h->kalfs, h->renor, -1},
                     {h->spec[2], h->spec[2], h->kalfs, h->renor, -1},
                     {h->spec[3], h->spec[3], h->kalfs, h->renor, -1}};
@@ -445,8 +471,8 @@ static int field_poten_merged(Handle *h) {
       double *out[3] = {h->intx, h->inty, h->intz};
       HE4_TRY(fft_c2r(h, 3, sp, out));
     }
-    k_alfa2<<<nblk(N), 256, 0, h->stream>>>(h->dxden, h->dyden, h->dzden, h->intx, h->inty, h->intz, h->falfs,
-                                           h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], N);
+    k_alfa2m<<<nblk(N), 256, 0, h->stream>>>(h->dxden, h->dyden, h->dzden, h->intx, h->inty, h->intz, h->denalf,
+                                            inv_den0s, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], N);
     HE4_LAUNCHED(h);
     const double *in[1] = {h->rtmp[0]};
     double2 *sp[1] = {h->spec[1]};

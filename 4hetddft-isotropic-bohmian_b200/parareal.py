@@ -261,21 +261,32 @@ class Parareal:
                                                renorm, C.c_void_p(out.data_ptr()),
                                                C.c_void_p(self.work.data_ptr()), sp), "he4_parareal_correct")
 
-    def _sequential(self, start):
+    def _sequential(self, start, resume=False):
         """Fallback: U[n+1] = F(U[n]) for n = start..S-1, one slice after
-        the other on the first handle."""
+        the other on the first handle.  resume: the first handle has just
+        integrated slice start-1 and still holds U[start] with its
+        predictor-corrector histories; the slices then continue that run
+        (one continuous integration, no starter steps at the boundaries)."""
         torch = self.torch
         torch.cuda.synchronize(self.dev)
         h = self.handles[0]
         for n in range(start, self.S):
-            h.set_state_device(*self.U[n].ptrs())
+            if not resume:
+                h.set_state_device(*self.U[n].ptrs())
             h.run(self.steps, self.dt)
             h.get_state_device(*self.U[n + 1].ptrs())
             self.fine_steps += self.steps
         torch.cuda.synchronize(self.dev)
 
+    def _rel_psi(self, a, b):
+        """||a.psi - b.psi|| / ||a.psi|| on the device."""
+        torch = self.torch
+        num = torch.linalg.vector_norm(a.psi - b.psi)
+        den = torch.linalg.vector_norm(a.psi)
+        return float((num / torch.clamp(den, min=1e-300)).item())
+
     def run(self, psi0, r0, v0, tol=1e-6, max_iter=None, fallback=True, contraction=0.5, first_change_max=0.1,
-            log=None):
+            judge_first=True, judge_max=None, log=None):
         """Returns a dict: iterations, per-iteration max relative psi change,
         wall seconds (device-synchronised), fine steps executed, and where the
         sequential fallback took over.  fallback: when an iteration does not
@@ -286,7 +297,15 @@ class Parareal:
         iteration's change is the coarse propagator's error over one slice as
         the fine propagator judges it; above first_change_max the remaining
         iterations cannot reach `tol` in fewer fine sweeps than the slices
-        left, so the fallback starts right away."""
+        left, so the fallback starts right away.  judge_first (with fallback):
+        the first iteration integrates slice 0 alone and compares its end with
+        the coarse prediction before integrating slices 1.. from predicted
+        states; a rejected coarse step then costs no speculative fine sweep
+        and the run is the sequential integration plus the coarse sweep.
+        judge_max is the largest accepted coarse error over that slice; its
+        default is tol, because the slices share one GPU here: a second
+        iteration would already cost more fine steps than the sequential
+        run, so speculation only pays when one iteration converges."""
         torch = self.torch
         max_iter = self.S if max_iter is None else max_iter
         t0 = time.perf_counter()
@@ -311,7 +330,20 @@ class Parareal:
         while k < max_iter:
             k += 1
             try:
-                self._fine(list(range(k - 1, self.S)))
+                if k == 1 and judge_first and fallback and self.S > 1:
+                    self._fine([0])
+                    err = self._rel_psi(self.F[1], self.Gold[1])
+                    if log:
+                        log(f"parareal judge: coarse step error over slice 0 {err:.3e}")
+                    if err > (tol if judge_max is None else judge_max):
+                        history.append(err)
+                        self.U[1].copy_(self.F[1])
+                        fallback_at = 1
+                        self._sequential(1, resume=True)
+                        break
+                    self._fine(list(range(1, self.S)))
+                else:
+                    self._fine(list(range(k - 1, self.S)))
             except He4Error as e:
                 if e.code != abi.HE4_E_NONFINITE:
                     raise
