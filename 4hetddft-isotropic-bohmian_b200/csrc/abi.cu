@@ -105,6 +105,7 @@ static void free_all(Handle *h) {
                   h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->bub, h->box,
                   h->k32[0], h->k32[1], h->k32[2], h->k32[3], h->dsym32};
   for (void *p : ptrs) cudaFree(p);
+  for (int i = 0; i < 9; i++) cudaFree(h->g32[i]);
   for (int i = 0; i < 8; i++) cudaFree(h->spec[i]);
   if (h->hscal) cudaFreeHost(h->hscal);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -194,6 +195,13 @@ static int create(const he4_params *pin, Handle *h) {
   int e = setup_kernels(h);
   h->p.vq_table = nullptr;
   HE4_TRY(e);
+  // (after setup_kernels, which sets the stencil width real32_ok reads)
+  h->real32 = real32_ok(h) ? 1 : 0;
+  if (h->real32)
+    for (int i = 0; i < 9; i++) {
+      HE4_TRY(dalloc(&h->g32[i], N));
+      HE4_CUDA_TRY(cudaMemsetAsync(h->g32[i], 0, sizeof(float) * N, h->stream));
+    }
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return HE4_OK;
 }
@@ -507,7 +515,10 @@ int he4_get_field(he4_handle *hh, int32_t which, double *out) {
   // fields a merged (time-step) evaluation leaves unwritten
   if (h->field_valid && !h->split_valid &&
       (which == HE4_F_UIMP || which == HE4_F_DELJ4 || which == HE4_F_UALPHAS || which == HE4_F_PENALTY ||
-       which == HE4_F_CORR || which == HE4_F_FALFS))
+       which == HE4_F_CORR || which == HE4_F_FALFS ||
+       (h->real32 && (which == HE4_F_DENCG || which == HE4_F_DENALF || which == HE4_F_DXDEN ||
+                      which == HE4_F_DYDEN || which == HE4_F_DZDEN || which == HE4_F_INTXALF ||
+                      which == HE4_F_INTYALF || which == HE4_F_INTZALF))))
     HE4_TRY(field_split_fields(h));
   switch (which) {
     case HE4_F_DEN: src = h->den; break;

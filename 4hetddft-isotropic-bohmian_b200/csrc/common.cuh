@@ -146,6 +146,11 @@ struct Handle {
   // FP32 copies of the kernels and of the derivative symbol
   int fp32 = 0;
   float *k32[4] = {nullptr, nullptr, nullptr, nullptr};  // wcgk, fvlj4, kalfs, vq
+  // FP32-convolution form with z-marching stencils: the merged evaluation
+  // keeps its intermediate real grids in float (dencg, denalf, the three
+  // density gradients, the three alpha_s integrals / products, s and lin)
+  int real32 = 0;
+  float *g32[9] = {nullptr};
   float *dsym32 = nullptr;
   // FP32 twin of one of the FP64 kernel arrays (nullptr for nullptr)
   const float *kern32(const double *k) const {
@@ -211,13 +216,18 @@ int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out);
 // x pass R2C whose input rows are formed on load from other grids:
 //   XLOAD_ALFA: in_f * (1 - aux0 * c0)     (falfs * d_f rho, term_alfa.f90:28-36)
 //   XLOAD_CORR: aux0 * aux1 * (c0 + c1 * aux1)  (poten.f90:62-64; `in` unused)
+// With real32 the rows `in` and the grids formed from (aux0 of ALFA, aux1 of
+// CORR) are float; aux0 of CORR (den) is always double.
 enum { XLOAD_PLAIN = 0, XLOAD_ALFA = 1, XLOAD_CORR = 2 };
 struct XLoad {
   int op = XLOAD_PLAIN;
-  const double *aux0 = nullptr, *aux1 = nullptr;
+  int real32 = 0;
+  const void *aux0 = nullptr, *aux1 = nullptr;
   double c0 = 0.0, c1 = 0.0;
 };
-int fft_r2c_load(Handle *h, int n, const double *const *in, double2 *const *out, const XLoad &ld);
+int fft_r2c_load(Handle *h, int n, const void *const *in, double2 *const *out, const XLoad &ld);
+// inverse transform into float real grids (FP32-convolution form)
+int fft_c2r_f32(Handle *h, int n, double2 *const *in, float *const *out);
 int fft_c2r(Handle *h, int n, double2 *const *in, double *const *out);
 int fft_y(Handle *h, int n, double2 *const *buf, bool inverse);
 // z pass: for each op, out = IFFT_z(coef * K * FFT_z(in)); K may be null (=1)
@@ -282,6 +292,8 @@ int field_forceimp(Handle *h, bool full);
 int field_forces(Handle *h, bool full);
 // the stencil passes of an evaluation (also timed by he4_bench_kernel)
 int launch_grad(Handle *h);
+// the merged evaluation may keep float intermediate grids (Handle::real32)
+bool real32_ok(const Handle *h);
 int launch_pot4_merged(Handle *h);
 // potenimp + poten + forceimp; marks the fields valid.  split = false takes
 // the merged form when the z length allows it.

@@ -483,10 +483,11 @@ void fft_plan_free(FftPlan &P) {
   }
 }
 
-// register-path x pass in the spectrum type C2 (the real grids stay FP64)
+// register-path x pass in the spectrum type C2; real grids FP64, or float
+// (ld.real32 / out32) in the merged evaluation of the FP32-convolution form
 template <typename C2>
-static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *const *cout, double2 *const *cin,
-                      double *const *rout, bool inverse, const BoxPair *box, const XLoad &ld) {
+static int x_pass_reg(Handle *h, int nb, const void *const *rin, double2 *const *cout, double2 *const *cin,
+                      void *const *rout, bool inverse, const BoxPair *box, const XLoad &ld, bool out32) {
   const FftPlan &P = h->fft;
   const long nrow = (long)P.ny * P.nz;
   XRegArgs<C2> a{};
@@ -510,38 +511,63 @@ static int x_pass_reg(Handle *h, int nb, const double *const *rin, double2 *cons
   HE4_REG_SWITCH(P.nx, P.n1[0], {
     constexpr int Pp = kRegThreads / N1_;
     dim3 grid((unsigned)((nrow + 2 * Pp - 1) / (2 * Pp)), nb);
-    if (inverse)
-      k_xc2r_reg<NN, N1_, C2><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
-    else if (ld.op == XLOAD_ALFA)
-      k_xr2c_reg<NN, N1_, C2, XLOAD_ALFA><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
-    else if (ld.op == XLOAD_CORR)
-      k_xr2c_reg<NN, N1_, C2, XLOAD_CORR><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
-    else
-      k_xr2c_reg<NN, N1_, C2><<<grid, kRegThreads, smem_x_reg<NN, N1_, C2>(), h->stream>>>(a);
+    const size_t sm = smem_x_reg<NN, N1_, C2>();
+    if constexpr (sizeof(C2) == 8) {
+      if (inverse && out32)
+        k_xc2r_reg<NN, N1_, C2, float><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (inverse)
+        k_xc2r_reg<NN, N1_, C2><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.real32 && ld.op == XLOAD_ALFA)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_ALFA, float><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.real32 && ld.op == XLOAD_CORR)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_CORR, float><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.real32)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_PLAIN, float><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.op == XLOAD_ALFA)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_ALFA><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.op == XLOAD_CORR)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_CORR><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else
+        k_xr2c_reg<NN, N1_, C2><<<grid, kRegThreads, sm, h->stream>>>(a);
+    } else {
+      if (out32 || ld.real32) {
+        set_error("float real grids need the FP32-convolution form");
+        return HE4_E_ARG;
+      }
+      if (inverse)
+        k_xc2r_reg<NN, N1_, C2><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.op == XLOAD_ALFA)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_ALFA><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else if (ld.op == XLOAD_CORR)
+        k_xr2c_reg<NN, N1_, C2, XLOAD_CORR><<<grid, kRegThreads, sm, h->stream>>>(a);
+      else
+        k_xr2c_reg<NN, N1_, C2><<<grid, kRegThreads, sm, h->stream>>>(a);
+    }
   });
   HE4_LAUNCHED(h);
   return HE4_OK;
 }
 
 // box (C2R only, register path): restrict to the rows of the force box
-static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *cout, double2 *const *cin,
-                  double *const *rout, bool inverse, const BoxPair *box = nullptr, const XLoad &ld = XLoad()) {
+// rin / rout: double grids, or float grids when ld.real32 (R2C) / out32 (C2R)
+static int x_pass_v(Handle *h, int n, const void *const *rin, double2 *const *cout, double2 *const *cin,
+                    void *const *rout, bool inverse, const BoxPair *box, const XLoad &ld, bool out32) {
   const FftPlan &P = h->fft;
   const long nrow = (long)P.ny * P.nz;
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
     const int nb = std::min(kMaxBatch, n - b0);
     if (reg_ok(P.nx)) {
-      const double *const *ri = rin ? rin + b0 : nullptr;
+      const void *const *ri = rin ? rin + b0 : nullptr;
       double2 *const *co = cout ? cout + b0 : nullptr;
       double2 *const *ci = cin ? cin + b0 : nullptr;
-      double *const *ro = rout ? rout + b0 : nullptr;
+      void *const *ro = rout ? rout + b0 : nullptr;
       if (h->fp32)
-        HE4_TRY(x_pass_reg<float2>(h, nb, ri, co, ci, ro, inverse, box, ld));
+        HE4_TRY(x_pass_reg<float2>(h, nb, ri, co, ci, ro, inverse, box, ld, out32));
       else
-        HE4_TRY(x_pass_reg<double2>(h, nb, ri, co, ci, ro, inverse, box, ld));
+        HE4_TRY(x_pass_reg<double2>(h, nb, ri, co, ci, ro, inverse, box, ld, out32));
       continue;
     }
-    if (ld.op != XLOAD_PLAIN) {
+    if (ld.op != XLOAD_PLAIN || ld.real32 || out32) {
       set_error("formed-on-load x pass needs a register-path axis length");
       return HE4_E_UNSUPPORTED;
     }
@@ -558,9 +584,9 @@ static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *co
     for (int i = 0; i < nb; i++) {
       if (inverse) {
         a.cin[i] = cin[b0 + i];
-        a.rout[i] = rout[b0 + i];
+        a.rout[i] = static_cast<double *>(rout[b0 + i]);
       } else {
-        a.rin[i] = rin[b0 + i];
+        a.rin[i] = static_cast<const double *>(rin[b0 + i]);
         a.cout[i] = cout[b0 + i];
       }
     }
@@ -572,6 +598,21 @@ static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *co
     HE4_LAUNCHED(h);
   }
   return HE4_OK;
+}
+
+static int x_pass(Handle *h, int n, const double *const *rin, double2 *const *cout, double2 *const *cin,
+                  double *const *rout, bool inverse, const BoxPair *box = nullptr) {
+  const void *ri[64];
+  void *ro[64];
+  if (n > 64) {
+    set_error("x pass of more than 64 fields");
+    return HE4_E_ARG;
+  }
+  for (int i = 0; i < n; i++) {
+    ri[i] = rin ? rin[i] : nullptr;
+    ro[i] = rout ? rout[i] : nullptr;
+  }
+  return x_pass_v(h, n, rin ? ri : nullptr, cout, cin, rout ? ro : nullptr, inverse, box, XLoad(), false);
 }
 
 // register-path transform of strided pencils in the spectrum type C2
@@ -676,9 +717,21 @@ int fft_r2c(Handle *h, int n, const double *const *in, double2 *const *out) {
   return HE4_OK;
 }
 
-int fft_r2c_load(Handle *h, int n, const double *const *in, double2 *const *out, const XLoad &ld) {
-  HE4_TRY(x_pass(h, n, in, out, nullptr, nullptr, false, nullptr, ld));
+int fft_r2c_load(Handle *h, int n, const void *const *in, double2 *const *out, const XLoad &ld) {
+  HE4_TRY(x_pass_v(h, n, in, out, nullptr, nullptr, false, nullptr, ld, false));
   HE4_TRY(fft_y(h, n, out, false));
+  return HE4_OK;
+}
+
+int fft_c2r_f32(Handle *h, int n, double2 *const *in, float *const *out) {
+  void *ro[64];
+  if (n > 64) {
+    set_error("x pass of more than 64 fields");
+    return HE4_E_ARG;
+  }
+  for (int i = 0; i < n; i++) ro[i] = out[i];
+  HE4_TRY(fft_y(h, n, in, true));
+  HE4_TRY(x_pass_v(h, n, nullptr, nullptr, in, ro, true, nullptr, XLoad(), true));
   return HE4_OK;
 }
 

@@ -104,22 +104,23 @@ struct XRegArgs {
   const C2 *tw;
   const BoxPair *box;  // non-null (C2R): only rows (y, z) inside the force box
   int ny, nz;
-  const double *rin[kRegBatch];
+  const void *rin[kRegBatch];  // double, or float (TI) for the R2C of real32 grids
   C2 *cout[kRegBatch];
   const C2 *cin[kRegBatch];
-  double *rout[kRegBatch];
-  XLoad ld;  // R2C: how input rows are formed
+  void *rout[kRegBatch];  // double, or float (TO) for the C2R into real32 grids
+  XLoad ld;               // R2C: how input rows are formed
 };
 
-// one input element of the R2C pass (XLoad; OP is the compile-time op)
-template <int OP>
-__device__ __forceinline__ double xload(const XLoad &ld, const double *__restrict__ in, long i) {
-  if (OP == XLOAD_ALFA) return (1.0 - ld.aux0[i] * ld.c0) * in[i];
+// one input element of the R2C pass (XLoad; OP is the compile-time op, TI
+// the type of the real32-able grids)
+template <int OP, typename TI>
+__device__ __forceinline__ double xload(const XLoad &ld, const TI *__restrict__ in, long i) {
+  if (OP == XLOAD_ALFA) return (1.0 - (double)static_cast<const TI *>(ld.aux0)[i] * ld.c0) * (double)in[i];
   if (OP == XLOAD_CORR) {
-    const double d = ld.aux0[i], c = ld.aux1[i];
+    const double d = static_cast<const double *>(ld.aux0)[i], c = (double)static_cast<const TI *>(ld.aux1)[i];
     return d * c * (ld.c0 + ld.c1 * c);
   }
-  return in[i];
+  return (double)in[i];
 }
 
 template <int N, typename C2>
@@ -419,7 +420,7 @@ inline size_t smem_zpipe() {
 }
 
 // x pass R2C: two real rows per complex pencil, Hermitian split
-template <int N, int N1, typename C2, int OP = XLOAD_PLAIN>
+template <int N, int N1, typename C2, int OP = XLOAD_PLAIN, typename TI = double>
 __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
   using T = typename regfft::Re<C2>::type;
   constexpr int N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
   __syncthreads();
   const int j1 = threadIdx.x % N1, p = threadIdx.x / N1;
   const long ra = (long)blockIdx.x * 2 * P + 2 * p, rb = ra + 1;
-  const double *in = a.rin[blockIdx.y];
+  const TI *in = static_cast<const TI *>(a.rin[blockIdx.y]);
   C2 *out = a.cout[blockIdx.y];
   // loads from clamped rows (unconditional, so they issue together), rows
   // past the end zeroed afterwards
@@ -438,8 +439,8 @@ __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
 #pragma unroll
   for (int j2 = 0; j2 < N2; j2++) {
     const int x = j1 + N1 * j2;
-    xa[j2] = xload<OP>(a.ld, in, rac * N + x);
-    xb[j2] = xload<OP>(a.ld, in, rbc * N + x);
+    xa[j2] = xload<OP, TI>(a.ld, in, rac * N + x);
+    xb[j2] = xload<OP, TI>(a.ld, in, rbc * N + x);
   }
   C2 v[N2];
 #pragma unroll
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
 }
 
 // x pass C2R: Hermitian extension of two half spectra, inverse, two rows
-template <int N, int N1, typename C2>
+template <int N, int N1, typename C2, typename TO = double>
 __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
   constexpr int N2 = N / N1, P = kRegThreads / N1, SP = N2 * (N1 + 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -485,7 +486,7 @@ __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
     if (!__syncthreads_or(ina || inb)) return;
   }
   const C2 *in = a.cin[blockIdx.y];
-  double *out = a.rout[blockIdx.y];
+  TO *out = static_cast<TO *>(a.rout[blockIdx.y]);
   C2 *Sp = S + p * SP;
   for (int k = j1; k < a.nxh; k += N1) {
     C2 X = ina ? in[ra * a.nxh + k] : regfft::mk<C2>(0, 0);
@@ -510,8 +511,8 @@ __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
 #pragma unroll
   for (int n2 = 0; n2 < N2; n2++) {
     const int x = j1 + N1 * n2;
-    if (ina) out[ra * N + x] = (double)v[n2].x * sc;
-    if (inb) out[rb * N + x] = (double)v[n2].y * sc;
+    if (ina) out[ra * N + x] = (TO)((double)v[n2].x * sc);
+    if (inb) out[rb * N + x] = (TO)((double)v[n2].y * sc);
   }
 }
 
@@ -630,6 +631,16 @@ inline int reg_attrs() {
                                     (int)smem_x_reg<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2, XLOAD_CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_x_reg<N, N1, C2>()));
+  if constexpr (sizeof(C2) == 8) {  // real32 grids exist in the FP32-convolution form only
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2, XLOAD_PLAIN, float>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N, N1, C2>()));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2, XLOAD_ALFA, float>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N, N1, C2>()));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2, XLOAD_CORR, float>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x_reg<N, N1, C2>()));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N, N1, C2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_x_reg<N, N1, C2>()));
+  }
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xc2r_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_x_reg<N, N1, C2>()));
   return HE4_OK;

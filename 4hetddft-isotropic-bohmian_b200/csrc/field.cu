@@ -37,14 +37,14 @@ struct OtArgs {
 // periodic index for i in [-n, 2n)
 __device__ __forceinline__ int wrap2(int i, int n) { return i < 0 ? i + n : (i >= n ? (i >= 2 * n ? i - 2 * n : i - n) : i); }
 
-// column values k0-M .. k0+ZB-1+M of f at (i, j)
-template <int M, int ZB>
-__device__ __forceinline__ void load_column(const double *__restrict__ f, const Geo &g, int i, int j, int k0,
+// column values k0-M .. k0+ZB-1+M of f at (i, j); f double or float
+template <int M, int ZB, typename T>
+__device__ __forceinline__ void load_column(const T *__restrict__ f, const Geo &g, int i, int j, int k0,
                                             double (&q)[ZB + 2 * M]) {
-  const double *col = f + (size_t)j * g.nx + i;
+  const T *col = f + (size_t)j * g.nx + i;
   const size_t ps = (size_t)g.ny * g.nx;
 #pragma unroll
-  for (int u = 0; u < ZB + 2 * M; u++) q[u] = __ldg(col + (size_t)wrap2(k0 - M + u, g.nz) * ps);
+  for (int u = 0; u < ZB + 2 * M; u++) q[u] = (double)__ldg(col + (size_t)wrap2(k0 - M + u, g.nz) * ps);
 }
 
 // Plane k of f into the tile s[8 + 2 HY][32 + 2 HX] around (i0, j0): the
@@ -52,26 +52,26 @@ __device__ __forceinline__ void load_column(const double *__restrict__ f, const 
 // otherwise), an x halo of HX cells on both sides of each row and a y halo
 // of HY rows above and below each column, all periodic.  Corners are not
 // filled (the stencils are one-dimensional).
-template <int HX, int HY>
-__device__ __forceinline__ void fill_tile(const double *__restrict__ f, const Geo &g, int i0, int j0, int k,
+template <int HX, int HY, typename T>
+__device__ __forceinline__ void fill_tile(const T *__restrict__ f, const Geo &g, int i0, int j0, int k,
                                           bool have, double centre, double (*s)[32 + 2 * HX]) {
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const double *plane = f + (size_t)k * g.ny * g.nx;
+  const T *plane = f + (size_t)k * g.ny * g.nx;
   const int gi = wrap2(i0 + tx, g.nx), gj = wrap2(j0 + ty, g.ny);
-  s[ty + HY][tx + HX] = have ? centre : __ldg(plane + (size_t)gj * g.nx + gi);
+  s[ty + HY][tx + HX] = have ? centre : (double)__ldg(plane + (size_t)gj * g.nx + gi);
   if (HX > 0 && tx < HX) {
-    s[ty + HY][tx] = __ldg(plane + (size_t)gj * g.nx + wrap2(i0 - HX + tx, g.nx));
-    s[ty + HY][tx + 32 + HX] = __ldg(plane + (size_t)gj * g.nx + wrap2(i0 + 32 + tx, g.nx));
+    s[ty + HY][tx] = (double)__ldg(plane + (size_t)gj * g.nx + wrap2(i0 - HX + tx, g.nx));
+    s[ty + HY][tx + 32 + HX] = (double)__ldg(plane + (size_t)gj * g.nx + wrap2(i0 + 32 + tx, g.nx));
   }
   if (HY > 0 && ty < HY) {
-    s[ty][tx + HX] = __ldg(plane + (size_t)wrap2(j0 - HY + ty, g.ny) * g.nx + gi);
-    s[ty + 8 + HY][tx + HX] = __ldg(plane + (size_t)wrap2(j0 + 8 + ty, g.ny) * g.nx + gi);
+    s[ty][tx + HX] = (double)__ldg(plane + (size_t)wrap2(j0 - HY + ty, g.ny) * g.nx + gi);
+    s[ty + 8 + HY][tx + HX] = (double)__ldg(plane + (size_t)wrap2(j0 + 8 + ty, g.ny) * g.nx + gi);
   }
 }
 
-template <int M, int ZB>
-__global__ void __launch_bounds__(256) k_grad_z(const double *__restrict__ f, double *dx, double *dy, double *dz,
-                                                Stencil st, Geo g) {
+template <int M, int ZB, typename TO = double>
+__global__ void __launch_bounds__(256) k_grad_z(const double *__restrict__ f, TO *dx, TO *dy, TO *dz, Stencil st,
+                                                Geo g) {
   __shared__ double s[8 + 2 * M][32 + 2 * M];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 8, k0 = blockIdx.z * ZB;
@@ -95,9 +95,9 @@ __global__ void __launch_bounds__(256) k_grad_z(const double *__restrict__ f, do
 #pragma unroll
     for (int u = -M; u <= M; u++) az += st.w1[2][u + M] * q[zz + M + u];
     const size_t t = ((size_t)k * g.ny + j) * g.nx + i;
-    dx[t] = ax;
-    dy[t] = ay;
-    dz[t] = az;
+    dx[t] = (TO)ax;
+    dy[t] = (TO)ay;
+    dz[t] = (TO)az;
   }
 }
 
@@ -108,10 +108,10 @@ __global__ void __launch_bounds__(256) k_grad_z(const double *__restrict__ f, do
 // planes then only wait for the L2-resident tile halos.
 constexpr int kZBp = 4;
 
-template <bool OTC, int M, int ZB>
-__global__ void __launch_bounds__(256) k_pot4_merged_z(const double *__restrict__ lin, const double *__restrict__ den,
-                                                       const double *__restrict__ dencg, const double *__restrict__ h0,
-                                                       const double *__restrict__ h1, const double *__restrict__ h2,
+template <bool OTC, int M, int ZB, typename TI = double>
+__global__ void __launch_bounds__(256) k_pot4_merged_z(const TI *__restrict__ lin, const double *__restrict__ den,
+                                                       const TI *__restrict__ dencg, const TI *__restrict__ h0,
+                                                       const TI *__restrict__ h1, const TI *__restrict__ h2,
                                                        double *pot4, Stencil st, Geo g, OtArgs a) {
   __shared__ double s0[8][32 + 2 * M];   // h0 with its x halo
   __shared__ double s1[8 + 2 * M][32];   // h1 with its y halo
@@ -127,12 +127,12 @@ __global__ void __launch_bounds__(256) k_pot4_merged_z(const double *__restrict_
     for (int zz = 0; zz < ZB; zz++) {
       const size_t t = (size_t)wrap2(k0 + zz, g.nz) * ps + (size_t)j * g.nx + i;
       if (OTC) {
-        c0[zz] = __ldg(h0 + t);
-        c1[zz] = __ldg(h1 + t);
+        c0[zz] = (double)__ldg(h0 + t);
+        c1[zz] = (double)__ldg(h1 + t);
       }
-      ld[zz] = __ldg(lin + t);
+      ld[zz] = (double)__ldg(lin + t);
       dd[zz] = __ldg(den + t);
-      dcg[zz] = __ldg(dencg + t);
+      dcg[zz] = (double)__ldg(dencg + t);
     }
   }
   const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0;
@@ -219,18 +219,20 @@ __global__ void k_alfa2(const double *__restrict__ dx, const double *__restrict_
 
 // k_alfa2 with falfs formed from denalf (merged evaluation, which does not
 // store falfs): f = 1 - denalf * (1/den0s)
-__global__ void k_alfa2m(const double *__restrict__ dx, const double *__restrict__ dy, const double *__restrict__ dz,
-                         const double *__restrict__ ix, const double *__restrict__ iy, const double *__restrict__ iz,
-                         const double *__restrict__ denalf, double inv_den0s, double *s, double *h0, double *h1,
-                         double *h2, size_t n) {
+// (T = float: the real32 grids of the FP32-convolution form; h_i may
+// overwrite int_i in place, each thread reading its point before writing it)
+template <typename T>
+__global__ void k_alfa2m(const T *dx, const T *dy, const T *dz, const T *ix, const T *iy, const T *iz,
+                         const T *denalf, double inv_den0s, T *s, T *h0, T *h1, T *h2, size_t n) {
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double a = ix[t], b = iy[t], c = iz[t];
-  s[t] = (dx[t] * a) + (dy[t] * b) + (dz[t] * c);
-  const double f = 1.0 - denalf[t] * inv_den0s;
-  h0[t] = f * a;
-  h1[t] = f * b;
-  h2[t] = f * c;
+  const double sx = (double)dx[t] * a, sy = (double)dy[t] * b, sz = (double)dz[t] * c;
+  const double f = 1.0 - (double)denalf[t] * inv_den0s;
+  s[t] = (T)((sx + sy) + sz);
+  h0[t] = (T)(f * a);
+  h1[t] = (T)(f * b);
+  h2[t] = (T)(f * c);
 }
 
 // ualphas = (u1/den0s + sum_i d_i h_i) * h2o2m4 * alphas ; pot4 += ualphas
@@ -331,6 +333,8 @@ static bool zmarch_ok(const Handle *h) {
 }
 
 static dim3 grid_z(const Geo &g, int zb = kZB) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + zb - 1) / zb); }
+
+bool real32_ok(const Handle *h) { return h->fp32 && zmarch_ok(h); }
 
 int launch_grad(Handle *h) {
   const Geo g = geo(h);
@@ -441,7 +445,7 @@ static int field_poten_merged(Handle *h) {
   // correlation source den*dencg*(cp4+cpp4*dencg) formed in the x pass,
   // x/y transform kept in spec[5]
   {
-    const double *in[1] = {h->den};
+    const void *in[1] = {h->den};
     double2 *sp[1] = {h->spec[5]};
     XLoad ld;
     ld.op = XLOAD_CORR;
@@ -457,7 +461,7 @@ static int field_poten_merged(Handle *h) {
     const double inv_den0s = 1.0 / h->p.den0s;
     {
       // g_i = falfs * d_i rho formed in the x pass (falfs is not stored)
-      const double *in[3] = {h->dxden, h->dyden, h->dzden};
+      const void *in[3] = {h->dxden, h->dyden, h->dzden};
       double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
       XLoad ld;
       ld.op = XLOAD_ALFA;
@@ -471,7 +475,7 @@ static int field_poten_merged(Handle *h) {
       double *out[3] = {h->intx, h->inty, h->intz};
       HE4_TRY(fft_c2r(h, 3, sp, out));
     }
-    k_alfa2m<<<nblk(N), 256, 0, h->stream>>>(h->dxden, h->dyden, h->dzden, h->intx, h->inty, h->intz, h->denalf,
+    k_alfa2m<double><<<nblk(N), 256, 0, h->stream>>>(h->dxden, h->dyden, h->dzden, h->intx, h->inty, h->intz, h->denalf,
                                             inv_den0s, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], N);
     HE4_LAUNCHED(h);
     const double *in[1] = {h->rtmp[0]};
@@ -488,8 +492,103 @@ static int field_poten_merged(Handle *h) {
   return HE4_OK;
 }
 
+// field_poten_merged of the FP32-convolution form with float intermediate
+// grids (Handle::real32): the same sequence; dencg, denalf, the gradients,
+// the alpha_s integrals (overwritten by the h_i), s and lin are float, den
+// and pot4 stay double, every pointwise and stencil sum is FP64.
+static int field_poten_merged_f32(Handle *h) {
+  const Geo g = geo(h);
+  const size_t N = h->N;
+  const OtArgs ot = ot_args(h);
+  const bool otc = (h->p.core4 == HE4_CORE_OTC);
+  float *dencg = h->g32[0], *denalf = h->g32[1], *gx = h->g32[2], *gy = h->g32[3], *gz = h->g32[4];
+  float *hv[3] = {h->g32[5], h->g32[6], h->g32[7]}, *sl = h->g32[8];
+  {
+    const double *in[1] = {h->den};
+    double2 *sp[1] = {h->spec[0]};
+    HE4_TRY(fft_r2c(h, 1, in, sp));
+  }
+  {
+    ZOp ops[2] = {{h->spec[0], h->spec[1], h->wcgk, h->renor, -1}, {h->spec[0], h->spec[3], h->kalfs, h->renor, -1}};
+    HE4_TRY(fft_z_conv(h, otc ? 2 : 1, ops));
+    double2 *sp[2] = {h->spec[1], h->spec[3]};
+    float *out[2] = {dencg, denalf};
+    HE4_TRY(fft_c2r_f32(h, otc ? 2 : 1, sp, out));
+  }
+  if (h->st.m == 3)
+    k_grad_z<3, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
+  else
+    k_grad_z<6, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
+  HE4_LAUNCHED(h);
+  {
+    const void *in[1] = {h->den};
+    double2 *sp[1] = {h->spec[5]};
+    XLoad ld;
+    ld.op = XLOAD_CORR;
+    ld.real32 = 1;
+    ld.aux0 = h->den;
+    ld.aux1 = dencg;
+    ld.c0 = ot.cp4;
+    ld.c1 = ot.cpp4;
+    HE4_TRY(fft_r2c_load(h, 1, in, sp, ld));
+  }
+  ZTerm terms[4] = {{h->spec[0], h->fvlj4, h->renor}, {h->spec[4], h->vq, h->renor}, {h->spec[5], h->wcgk, h->renor},
+                    {h->spec[1], h->kalfs, h->renor * h->p.h2o2m4 * h->p.alphas / h->p.den0s}};
+  if (otc) {
+    const double inv_den0s = 1.0 / h->p.den0s;
+    {
+      const void *in[3] = {gx, gy, gz};
+      double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
+      XLoad ld;
+      ld.op = XLOAD_ALFA;
+      ld.real32 = 1;
+      ld.aux0 = denalf;
+      ld.c0 = inv_den0s;
+      HE4_TRY(fft_r2c_load(h, 3, in, sp, ld));
+      ZOp ops[3] = {{h->spec[1], h->spec[1], h->kalfs, h->renor, -1},
+                    {h->spec[2], h->spec[2], h->kalfs, h->renor, -1},
+                    {h->spec[3], h->spec[3], h->kalfs, h->renor, -1}};
+      HE4_TRY(fft_z_conv(h, 3, ops));
+      HE4_TRY(fft_c2r_f32(h, 3, sp, hv));
+    }
+    // h_i over int_i in place; s into sl
+    k_alfa2m<float><<<nblk(N), 256, 0, h->stream>>>(gx, gy, gz, hv[0], hv[1], hv[2], denalf, inv_den0s, sl, hv[0],
+                                                   hv[1], hv[2], N);
+    HE4_LAUNCHED(h);
+    const void *in[1] = {sl};
+    double2 *sp[1] = {h->spec[1]};
+    XLoad ld;
+    ld.real32 = 1;
+    HE4_TRY(fft_r2c_load(h, 1, in, sp, ld));
+  }
+  HE4_TRY(fft_z_sum(h, otc ? 4 : 3, terms, h->spec[2]));
+  {
+    double2 *sp[1] = {h->spec[2]};
+    float *out[1] = {sl};  // lin (s is consumed)
+    HE4_TRY(fft_c2r_f32(h, 1, sp, out));
+  }
+  const float *h0 = otc ? hv[0] : nullptr, *h1 = otc ? hv[1] : nullptr, *h2 = otc ? hv[2] : nullptr;
+  if (h->st.m == 3) {
+    if (otc)
+      k_pot4_merged_z<true, 3, kZBp, float><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(sl, h->den, dencg, h0, h1,
+                                                                                       h2, h->pot4, h->st, g, ot);
+    else
+      k_pot4_merged_z<false, 3, kZBp, float><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(sl, h->den, dencg, h0, h1,
+                                                                                        h2, h->pot4, h->st, g, ot);
+  } else {
+    if (otc)
+      k_pot4_merged_z<true, 6, kZBp, float><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(sl, h->den, dencg, h0, h1,
+                                                                                       h2, h->pot4, h->st, g, ot);
+    else
+      k_pot4_merged_z<false, 6, kZBp, float><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(sl, h->den, dencg, h0, h1,
+                                                                                        h2, h->pot4, h->st, g, ot);
+  }
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
+
 int field_poten(Handle *h, bool split, double *pot4) {
-  if (!split) return field_poten_merged(h);
+  if (!split) return h->real32 ? field_poten_merged_f32(h) : field_poten_merged(h);
   const Geo g = geo(h);
   const size_t N = h->N;
   const OtArgs ot = ot_args(h);
