@@ -52,6 +52,26 @@ template <typename C2>
 __device__ __forceinline__ C2 add(C2 a, C2 b) { return mk<C2>(a.x + b.x, a.y + b.y); }
 template <typename C2>
 __device__ __forceinline__ C2 sub(C2 a, C2 b) { return mk<C2>(a.x - b.x, a.y - b.y); }
+// FP32: both components in one packed instruction (sm_100 f32x2 arithmetic;
+// the same round-to-nearest sums as the scalar form)
+template <>
+__device__ __forceinline__ float2 add<float2>(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2,%3};\n\tmov.b64 rb, {%4,%5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0,%1}, rd;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+template <>
+__device__ __forceinline__ float2 sub<float2>(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2,%3};\n\tmov.b64 rb, {%4,%5};\n\t"
+      "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0,%1}, rd;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
 template <typename C2>
 __device__ __forceinline__ C2 scale(C2 a, typename Re<C2>::type s) { return mk<C2>(a.x * s, a.y * s); }
 template <typename C2>
