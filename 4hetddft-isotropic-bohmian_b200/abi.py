@@ -20,6 +20,7 @@ HE4_CORE_OTC = 1
 HE4_POT_TABLE = 0
 HE4_POT_MORSE = 1
 HE4_POT_NULL = 2
+HE4_POT_RTABLE = 3
 
 HE4_PREC_FP64 = 0
 HE4_PREC_FP32CONV = 1
@@ -65,6 +66,9 @@ class He4Params(C.Structure):
         ("lambdah", C.c_double), ("tzmean", C.c_double), ("tzsurf", C.c_double),
         ("precision", C.c_int32),
         ("device", C.c_int32),
+        ("vr_table", C.POINTER(C.c_double)),
+        ("n_vr", C.c_int32),
+        ("vr_r0", C.c_double), ("vr_dr", C.c_double),
     ]
 
 

@@ -63,7 +63,8 @@ static int check_params(const he4_params *p) {
     set_error("invalid ironx, mimpur or box size");
     return HE4_E_ARG;
   }
-  if (p->pot_kind != HE4_POT_TABLE && p->pot_kind != HE4_POT_MORSE && p->pot_kind != HE4_POT_NULL) {
+  if (p->pot_kind != HE4_POT_TABLE && p->pot_kind != HE4_POT_MORSE && p->pot_kind != HE4_POT_NULL &&
+      p->pot_kind != HE4_POT_RTABLE) {
     set_error("unknown pot_kind %d", p->pot_kind);
     return HE4_E_ARG;
   }
@@ -115,6 +116,7 @@ static int create(const he4_params *pin, Handle *h) {
   HE4_TRY(check_params(pin));
   h->p = *pin;
   h->p.vq_table = nullptr;
+  h->p.vr_table = nullptr;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("no CUDA device");
@@ -191,9 +193,11 @@ static int create(const he4_params *pin, Handle *h) {
   HE4_TRY(impurity_reset_box(h));
   he4_params with_table = p;
   with_table.vq_table = pin->vq_table;
+  with_table.vr_table = pin->vr_table;
   h->p = with_table;
   int e = setup_kernels(h);
   h->p.vq_table = nullptr;
+  h->p.vr_table = nullptr;
   HE4_TRY(e);
   // (after setup_kernels, which sets the stencil width real32_ok reads)
   h->real32 = real32_ok(h) ? 1 : 0;

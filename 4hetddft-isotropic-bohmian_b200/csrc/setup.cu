@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <cmath>
+
 #include "common.cuh"
 #include "reduce.cuh"
 
@@ -241,9 +243,53 @@ __global__ void k_kspace(KArgs a, double *pmod, double *wcgk, double *fvlj4, dou
 // ---------------------------------------------------------------------------
 // FT_V_spline
 // ---------------------------------------------------------------------------
-static double pair_pot(const he4_params &p, double r) {
+// spline of a caller-sampled V(r) (HE4_POT_RTABLE): uniform nodes
+// r_i = r0 + i dr, natural end conditions, global-form coefficients
+struct RTable {
+  int n = 0;
+  double r0 = 0.0, dr = 0.0, rend = 0.0;
+  std::vector<double> A, B, C, D;
+};
+
+static int rtable_build(const he4_params &p, RTable *t) {
+  if (!p.vr_table || p.n_vr < 4 || !(p.vr_dr > 0.0) || !(p.vr_r0 <= p.r_cutoff + 1e-8)) {
+    set_error("HE4_POT_RTABLE needs vr_table, n_vr >= 4, vr_dr > 0 and vr_r0 <= r_cutoff");
+    return HE4_E_ARG;
+  }
+  const int n = p.n_vr;
+  std::vector<double> x(n), y(n);
+  for (int i = 0; i < n; i++) {
+    x[i] = p.vr_r0 + (double)i * p.vr_dr;
+    y[i] = p.vr_table[i];
+    if (!std::isfinite(y[i])) {
+      set_error("vr_table[%d] is not finite", i);
+      return HE4_E_ARG;
+    }
+  }
+  t->n = n;
+  t->r0 = p.vr_r0;
+  t->dr = p.vr_dr;
+  t->rend = x[n - 1];
+  t->A.resize(n);
+  t->B.resize(n);
+  t->C.resize(n);
+  t->D.resize(n);
+  return spline_global(x.data(), y.data(), t->A.data(), t->B.data(), t->C.data(), t->D.data(), 0.0, 0.0, n);
+}
+
+static double rtable_eval(const RTable &t, double r) {
+  if (r > t.rend) return 0.0;
+  int k = (int)((r - t.r0) / t.dr);
+  if (k < 0) k = 0;
+  if (k > t.n - 2) k = t.n - 2;
+  return t.A[k] + r * (t.B[k] + r * (t.C[k] + r * t.D[k]));
+}
+
+// Select_Pot conventions (V_impur.f90:84-935): r < r_cutoff -> umax
+static double pair_pot(const he4_params &p, const RTable *t, double r) {
   if (p.pot_kind == HE4_POT_NULL) return 0.0;
   if (r < p.r_cutoff) return p.umax;
+  if (p.pot_kind == HE4_POT_RTABLE) return rtable_eval(*t, r);
   const double e = 1.0 - exp(-p.morse_alpha * (r - p.morse_re));
   return p.morse_d * (e * e - 1.0);
 }
@@ -384,14 +430,18 @@ static int build_vq(Handle *h, double qmax, double hq) {
     set_error("Vq table needs at least 4 q points (nq=%d)", P.nq);
     return HE4_E_ARG;
   }
+  RTable tab;
+  if (P.pot_kind == HE4_POT_RTABLE) HE4_TRY(rtable_build(P, &tab));
+  const RTable *t = &tab;
   std::vector<double> x(N), y(N), A(N), B(N), C(N), D(N);
   const double X1 = P.r_cutoff + eps, XN = r_max;
-  const double S1 = (pair_pot(P, X1) - 2.0 * pair_pot(P, X1 + dr) + pair_pot(P, X1 + dr + dr)) / (dr * dr);
-  const double Sn = (pair_pot(P, XN - dr) - 2.0 * pair_pot(P, XN) + pair_pot(P, XN + dr)) / (dr * dr);
+  const double S1 =
+      (pair_pot(P, t, X1) - 2.0 * pair_pot(P, t, X1 + dr) + pair_pot(P, t, X1 + dr + dr)) / (dr * dr);
+  const double Sn = (pair_pot(P, t, XN - dr) - 2.0 * pair_pot(P, t, XN) + pair_pot(P, t, XN + dr)) / (dr * dr);
   const double hr = (XN - X1) / (N - 1);
   for (int i = 0; i < N; i++) {
     x[i] = (double)i * hr + X1;
-    y[i] = pair_pot(P, x[i]);
+    y[i] = pair_pot(P, t, x[i]);
   }
   HE4_TRY(spline_global(x.data(), y.data(), A.data(), B.data(), C.data(), D.data(), S1, Sn, N));
   DevBuf<double> dx, dA, dB, dC, dD, dv;

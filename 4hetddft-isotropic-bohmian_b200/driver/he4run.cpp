@@ -88,6 +88,7 @@ struct Run {
   std::vector<std::complex<double>> psi;
   std::vector<double> rimp, vimp, aimp;
   std::vector<double> vq;  // tabulated Vq (vqfile)
+  std::vector<double> vr;  // sampled V(r) (vrfile)
   int npar = 0, n4 = 300, niter = 0, iter0 = 0, pener = 50, pcurr = 0, icurr = 0;
   bool lrk = false, binary = false;
   // spherical bubble radius of the pener block (DFT4He3d.f90:126-135,698-760)
@@ -147,6 +148,26 @@ void load_input(Run &r, const std::string &text) {
     for (size_t i = 0; i < H; i++)
       if (!(f >> r.vq[i])) die("vqfile holds fewer than (nx/2+1)*ny*nz values");
     p.vq_table = r.vq.data();
+  } else if (nl.has("vrfile")) {
+    // any Select_Pot entry sampled on a uniform r grid: lines "r V(r)" from
+    // r_cutoff on; the library splines and Fourier-transforms it
+    std::ifstream f(nl.str("vrfile", ""));
+    if (!f) die("cannot open vrfile");
+    std::vector<double> rs;
+    double a, b;
+    while (f >> a >> b) {
+      rs.push_back(a);
+      r.vr.push_back(b);
+    }
+    if (rs.size() < 4) die("vrfile holds fewer than 4 (r, V) pairs");
+    const double dr = (rs.back() - rs.front()) / (double)(rs.size() - 1);
+    for (size_t i = 1; i < rs.size(); i++)
+      if (std::fabs(rs[i] - rs[i - 1] - dr) > 1e-6 * dr) die("vrfile r values are not uniformly spaced");
+    p.pot_kind = HE4_POT_RTABLE;
+    p.vr_table = r.vr.data();
+    p.n_vr = (int32_t)r.vr.size();
+    p.vr_r0 = rs.front();
+    p.vr_dr = dr;
   } else if (selec == "morse") {
     p.pot_kind = HE4_POT_MORSE;
     p.morse_d = nl.real("morse_d", 10.0);

@@ -46,7 +46,10 @@ enum {
   HE4_POT_TABLE = 0, /* caller supplies Vq on the half-spectrum grid        */
   HE4_POT_MORSE = 1, /* V(r)=D[(1-exp(-a(r-re)))^2-1], r<r_cutoff -> umax,  */
                      /* transformed by the FT_V_spline procedure           */
-  HE4_POT_NULL = 2   /* V = 0 ('null' entry of Select_Pot)                  */
+  HE4_POT_NULL = 2,  /* V = 0 ('null' entry of Select_Pot)                  */
+  HE4_POT_RTABLE = 3 /* caller samples V(r) (any Select_Pot entry) on a     */
+                     /* uniform r grid; splined, r<r_cutoff -> umax, 0 past */
+                     /* the last point, transformed by FT_V_spline          */
 };
 
 /* Arithmetic of the convolution FFTs and the pointwise potential assembly.
@@ -82,6 +85,12 @@ typedef struct he4_params {
   double lambdah, tzmean, tzsurf;
   int32_t precision;
   int32_t device; /* CUDA device ordinal                                   */
+  /* HE4_POT_RTABLE: V(r) in K at r_i = vr_r0 + i vr_dr, i < n_vr; needs
+   * n_vr >= 4, vr_dr > 0 and vr_r0 <= r_cutoff (the table covers the
+   * potential from the cutoff on).  Borrowed for he4_create only. */
+  const double *vr_table;
+  int32_t n_vr;
+  double vr_r0, vr_dr;
 } he4_params;
 
 /* Energies of energy.f90:51-124, same names as module energies. */

@@ -518,10 +518,43 @@ static int findi(const double *x, double xc, int n) {
   return i;
 }
 
+/* A caller-sampled V(r) (HE4_POT_RTABLE): natural cubic spline through
+ * r_i = r0 + i dr in Maron's global form; zero past the last node. */
+typedef struct {
+  int n;
+  double r0, dr, rend;
+  double *a, *b, *c, *d;
+} rtab;
+
+static int rtab_build(const he4_params *p, rtab *t) {
+  memset(t, 0, sizeof(*t));
+  if (!p->vr_table || p->n_vr < 4 || !(p->vr_dr > 0.0) || !(p->vr_r0 <= p->r_cutoff + 1e-8)) return HE4_E_ARG;
+  int n = p->n_vr;
+  double *x = malloc(sizeof(double) * n);
+  t->a = malloc(sizeof(double) * n); t->b = malloc(sizeof(double) * n);
+  t->c = malloc(sizeof(double) * n); t->d = malloc(sizeof(double) * n);
+  for (int i = 0; i < n; i++) x[i] = p->vr_r0 + (double)i * p->vr_dr;
+  t->n = n; t->r0 = p->vr_r0; t->dr = p->vr_dr; t->rend = x[n - 1];
+  int e = ora_spline(x, p->vr_table, t->a, t->b, t->c, t->d, 0.0, 0.0, n);
+  free(x);
+  return e;
+}
+
+static void rtab_free(rtab *t) { free(t->a); free(t->b); free(t->c); free(t->d); }
+
+static double rtab_eval(const rtab *t, double r) {
+  if (r > t->rend) return 0.0;
+  int k = (int)((r - t->r0) / t->dr);
+  if (k < 0) k = 0;
+  if (k > t->n - 2) k = t->n - 2;
+  return t->a[k] + r * (t->b[k] + r * (t->c[k] + r * t->d[k]));
+}
+
 /* Select_Pot conventions (V_impur.f90:84-935): r < r_cutoff -> umax. */
-static double pair_pot(const he4_params *p, double r) {
+static double pair_pot(const he4_params *p, const rtab *t, double r) {
   if (p->pot_kind == HE4_POT_NULL) return 0.0;
   if (r < p->r_cutoff) return p->umax;
+  if (p->pot_kind == HE4_POT_RTABLE) return rtab_eval(t, r);
   double e = 1.0 - exp(-p->morse_alpha * (r - p->morse_re));
   return p->morse_d * (e * e - 1.0);
 }
@@ -543,15 +576,22 @@ static int ft_v_spline_build(const he4_params *P, double pmax, double hp, qsplin
   double *x = malloc(sizeof(double) * N), *y = malloc(sizeof(double) * N);
   double *A = malloc(sizeof(double) * N), *B = malloc(sizeof(double) * N);
   double *C = malloc(sizeof(double) * N), *D = malloc(sizeof(double) * N);
+  rtab T;
+  memset(&T, 0, sizeof(T));
+  if (P->pot_kind == HE4_POT_RTABLE) {
+    int e0 = rtab_build(P, &T);
+    if (e0) { rtab_free(&T); return e0; }
+  }
   double X1 = P->r_cutoff + eps, XN = r_max;
   double r0 = X1, r1 = r0 + dr, r2 = r1 + dr;
-  double S1 = (pair_pot(P, r0) - 2.0 * pair_pot(P, r1) + pair_pot(P, r2)) / (dr * dr);
-  double Sn = (pair_pot(P, XN - dr) - 2.0 * pair_pot(P, XN) + pair_pot(P, XN + dr)) / (dr * dr);
+  double S1 = (pair_pot(P, &T, r0) - 2.0 * pair_pot(P, &T, r1) + pair_pot(P, &T, r2)) / (dr * dr);
+  double Sn = (pair_pot(P, &T, XN - dr) - 2.0 * pair_pot(P, &T, XN) + pair_pot(P, &T, XN + dr)) / (dr * dr);
   double h = (XN - X1) / (N - 1);
   for (int i = 0; i < N; i++) {
     x[i] = (double)i * h + X1;
-    y[i] = pair_pot(P, x[i]);
+    y[i] = pair_pot(P, &T, x[i]);
   }
+  rtab_free(&T);
   int e = ora_spline(x, y, A, B, C, D, S1, Sn, N);
   if (e) return e;
   double *Vpp = malloc(sizeof(double) * np), *Pp = malloc(sizeof(double) * np);
@@ -763,6 +803,7 @@ int ora_create(const he4_params *pin, ora_state **out) {
   ora_state *s = xalloc(sizeof(*s));
   s->p = *p;
   s->p.vq_table = NULL;
+  s->p.vr_table = NULL;
   int nx = p->nx, ny = p->ny, nz = p->nz;
   s->nx = nx; s->ny = ny; s->nz = nz; s->nxh = nx / 2 + 1;
   s->N = (size_t)nx * ny * nz;

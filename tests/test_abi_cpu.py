@@ -47,9 +47,10 @@ def test_struct_layout_matches_header(pkg):
 #include <stddef.h>
 #include "he4_tddft.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(he4_params), sizeof(he4_energies),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(he4_params), sizeof(he4_energies),
          offsetof(he4_params, vq_table), offsetof(he4_params, lambdah),
-         offsetof(he4_params, device), offsetof(he4_params, nq));
+         offsetof(he4_params, device), offsetof(he4_params, nq),
+         offsetof(he4_params, vr_table), offsetof(he4_params, vr_dr));
   return 0;
 }
 """
@@ -60,7 +61,8 @@ int main(void) {
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
         got = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
     P, E = pkg.abi.He4Params, pkg.abi.He4Energies
-    want = [C.sizeof(P), C.sizeof(E), P.vq_table.offset, P.lambdah.offset, P.device.offset, P.nq.offset]
+    want = [C.sizeof(P), C.sizeof(E), P.vq_table.offset, P.lambdah.offset, P.device.offset, P.nq.offset,
+            P.vr_table.offset, P.vr_dr.offset]
     assert got == want
 
 
@@ -68,7 +70,8 @@ def test_defaults_match_reference_modules(pkg, lib):
     p = pkg.params_default()
     q = pkg.abi.default_params()
     for name, _ in pkg.abi.He4Params._fields_:
-        if name == "vq_table":
+        if name in ("vq_table", "vr_table"):
+            assert not getattr(p, name) and not getattr(q, name), name  # null pointers
             continue
         assert getattr(p, name) == getattr(q, name), name
     # modules.f90:15,19,88-90,130-139,144,205-210

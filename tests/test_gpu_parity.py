@@ -62,6 +62,27 @@ def test_kspace_kernels(pkg, c1):
         assert np.mean(gv == vq) > 0.99
 
 
+def test_vq_from_sampled_potential(pkg, ora):
+    """HE4_POT_RTABLE: FT_V_spline on the device from a caller-sampled V(r)
+    equals the oracle's to one FP32 ulp, and the analytic entry it samples."""
+    import test_oracle_pins as pins
+    p = pkg.workloads.make_params(32, 0.6, 8, nq=400)
+    q, keep = pins.rtable_params(pkg, p)
+    o = ora.Oracle(q)
+    want = o.get_kernel("vq")
+    o.close()
+    with pkg.He4Step(q) as g:
+        got = g.get_kernel("vq")
+    with pkg.He4Step(p) as g:
+        morse = g.get_kernel("vq")
+    ulp = np.spacing(np.abs(want).astype(np.float32)).astype(np.float64)
+    assert np.all(np.abs(got - want) <= ulp)
+    assert np.max(np.abs(got - morse)) <= 2e-6 * np.max(np.abs(morse))
+    q.vr_r0 = p.r_cutoff + 0.5
+    with pytest.raises(pkg.He4Error):
+        pkg.He4Step(q)
+
+
 @pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 80), (48, 40, 30)])
 def test_fft_against_numpy_and_cufft(pkg, shape):
     import ctypes as C
@@ -131,6 +152,37 @@ def test_steps_parity(pkg, c1):
         ng = np.sum(g.get_field("den")) * dxyz
         no = np.sum(o.get_field("den")) * dxyz
         assert abs(ng - no) <= 1e-10 * no
+
+
+def test_steps_parity_absorbing_layer(pkg, ora, c1):
+    """Lambdah != 0: timec = (Lambdah (1 + tanh((z - tzmean)/tzsurf)), 1)
+    (DFT4He3d.f90:773-782, real part rounded to real(4)) multiplies H psi in
+    every RK stage and PC step; 3 RK + 5 PC steps against the oracle."""
+    p, psi, r, v, o0, vq = c1
+    q = pkg.abi.He4Params.from_buffer_copy(p)
+    q.lambdah, q.tzmean, q.tzsurf = 0.05, 12.0, 2.0
+    dt = pkg.workloads.deltat_fs(1.0)
+    o = ora.Oracle(q)
+    o.set_state(psi, r, v)
+    eo, mo = o.run(8, dt)
+    with gpu_with_table(pkg, q, vq) as g:
+        g.set_state(psi, r, v)
+        eg, mg = g.run(8, dt)
+        assert np.allclose(eg[3:], eo[3:], rtol=1e-8, atol=0)
+        assert np.allclose(mg, mo, rtol=1e-9, atol=1e-9 * np.abs(mo).max())
+        psg = g.get_state()[0]
+        pso = o.get_state()[0]
+        assert rel(psg, pso) < 1e-10
+        Eg, Eo = g.energy(), o.energy()
+        for k in Eo:
+            assert abs(Eg[k] - Eo[k]) <= 1e-10 * max(abs(Eo[k]), 1e-30), (k, Eg[k], Eo[k])
+    o.close()
+    # the layer damps: the norm decays only where tanh is switched on
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        g.run(8, dt)
+        n_plain = np.sum(np.abs(g.get_state()[0]) ** 2)
+    assert np.sum(np.abs(psg) ** 2) != n_plain
 
 
 def test_run_equals_single_steps_and_is_deterministic(pkg, c1):

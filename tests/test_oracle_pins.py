@@ -157,6 +157,35 @@ def test_vq_matches_quadrature_of_capped_morse(pkg, small):
     assert np.array_equal(vq, vq.astype(np.float32).astype(np.float64))
 
 
+def rtable_params(pkg, p, dr=0.005, rend=80.0):
+    """The capped Morse entry of p sampled as a V(r) table from r_cutoff."""
+    import ctypes as C
+    r = p.r_cutoff + dr * np.arange(int((rend - p.r_cutoff) / dr) + 1)
+    v = np.ascontiguousarray(p.morse_d * ((1.0 - np.exp(-p.morse_alpha * (r - p.morse_re))) ** 2 - 1.0))
+    q = pkg.abi.He4Params.from_buffer_copy(p)
+    q.pot_kind = pkg.abi.HE4_POT_RTABLE
+    q.vr_table = v.ctypes.data_as(C.POINTER(C.c_double))
+    q.n_vr = v.size
+    q.vr_r0 = p.r_cutoff
+    q.vr_dr = dr
+    return q, v
+
+
+def test_vq_from_a_sampled_potential_matches_the_analytic_entry(pkg, ora, small):
+    """HE4_POT_RTABLE: the same FT_V_spline procedure from a spline of
+    sampled V(r) values gives the analytic entry's Vq (both FP32-rounded)."""
+    p, o = small
+    q, keep = rtable_params(pkg, p)
+    o2 = ora.Oracle(q)
+    a, b = o.get_kernel("vq"), o2.get_kernel("vq")
+    o2.close()
+    assert np.max(np.abs(a - b)) <= 2e-6 * np.max(np.abs(a))
+    # a table that starts above the cutoff does not cover the potential
+    q.vr_r0 = p.r_cutoff + 0.5
+    with pytest.raises(ora.OracleError):
+        ora.Oracle(q)
+
+
 def test_periodic_stencils_match_fourier_symbol(pkg, ora, small):
     p, o = small
     n = p.nx
