@@ -78,7 +78,7 @@ def build_driver(verbose=False):
     linked against libhe4b200.so next to it."""
     srcs = [os.path.join(HERE, "driver", f) for f in DRIVER_SOURCES]
     cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", *srcs, "-o", DRIVER + ".tmp",
-           "-L" + HERE, "-lhe4b200", "-Wl,-rpath,$ORIGIN"]
+           "-L" + HERE, "-lhe4b200", "-Wl,-rpath,$ORIGIN", "-pthread"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

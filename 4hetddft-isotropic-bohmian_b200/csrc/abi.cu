@@ -107,6 +107,12 @@ static void free_all(Handle *h) {
                   h->k32[0], h->k32[1], h->k32[2], h->k32[3], h->dsym32};
   for (void *p : ptrs) cudaFree(p);
   for (int i = 0; i < 9; i++) cudaFree(h->g32[i]);
+  if (h->snap_stream) cudaStreamSynchronize(h->snap_stream);
+  cudaFree(h->snap_dev);
+  if (h->snap_host) cudaFreeHost(h->snap_host);
+  if (h->snap_taken) cudaEventDestroy(h->snap_taken);
+  if (h->snap_done) cudaEventDestroy(h->snap_done);
+  if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
   for (int i = 0; i < 8; i++) cudaFree(h->spec[i]);
   if (h->hscal) cudaFreeHost(h->hscal);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -333,6 +339,57 @@ int he4_get_state(he4_handle *hh, double *psi, double *rimp, double *vimp, doubl
   if (vimp) HE4_CUDA_TRY(cudaMemcpyAsync(vimp, h->vimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
   if (aimp) HE4_CUDA_TRY(cudaMemcpyAsync(aimp, h->aimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HE4_OK;
+}
+
+// Checkpoint snapshot: a device-to-device copy of the state on the
+// handle's stream, then a device-to-host copy on a copy stream that
+// overlaps the time steps enqueued after it.
+int he4_snapshot_begin(he4_handle *hh) {
+  HANDLE_OR_FAIL(hh);
+  NEED_STATE(h);
+  const size_t P3 = 3 * (size_t)h->npar, n = 2 * h->N + 3 * P3;
+  if (h->snap_pending) {  // one snapshot in flight at a time
+    HE4_CUDA_TRY(cudaEventSynchronize(h->snap_done));
+    h->snap_pending = 0;
+  }
+  if (!h->snap_dev) {
+    HE4_CUDA_TRY(cudaMalloc((void **)&h->snap_dev, sizeof(double) * n));
+    HE4_CUDA_TRY(cudaMallocHost((void **)&h->snap_host, sizeof(double) * n));
+    HE4_CUDA_TRY(cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+    HE4_CUDA_TRY(cudaEventCreateWithFlags(&h->snap_taken, cudaEventDisableTiming));
+    HE4_CUDA_TRY(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+  }
+  double *d = h->snap_dev;
+  HE4_CUDA_TRY(cudaMemcpyAsync(d, h->psi, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
+  d += 2 * h->N;
+  const double *parts[3] = {h->rimp, h->vimp, h->aimp};
+  for (int a = 0; a < 3; a++)
+    HE4_CUDA_TRY(cudaMemcpyAsync(d + a * P3, parts[a], sizeof(double) * P3, cudaMemcpyDeviceToDevice, h->stream));
+  HE4_CUDA_TRY(cudaEventRecord(h->snap_taken, h->stream));
+  HE4_CUDA_TRY(cudaStreamWaitEvent(h->snap_stream, h->snap_taken, 0));
+  HE4_CUDA_TRY(cudaMemcpyAsync(h->snap_host, h->snap_dev, sizeof(double) * n, cudaMemcpyDeviceToHost, h->snap_stream));
+  HE4_CUDA_TRY(cudaEventRecord(h->snap_done, h->snap_stream));
+  h->snap_pending = 1;
+  return HE4_OK;
+}
+
+int he4_snapshot_wait(he4_handle *hh, const double **psi, const double **rimp, const double **vimp,
+                      const double **aimp) {
+  HANDLE_OR_FAIL(hh);
+  if (!h->snap_pending) {
+    set_error("he4_snapshot_wait without a snapshot in flight");
+    return HE4_E_STATE;
+  }
+  HE4_CUDA_TRY(cudaEventSynchronize(h->snap_done));
+  h->snap_pending = 0;
+  const size_t P3 = 3 * (size_t)h->npar;
+  const double *b = h->snap_host;
+  if (psi) *psi = b;
+  b += 2 * h->N;
+  if (rimp) *rimp = b;
+  if (vimp) *vimp = b + P3;
+  if (aimp) *aimp = b + 2 * P3;
   return HE4_OK;
 }
 

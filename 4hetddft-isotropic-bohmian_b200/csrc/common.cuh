@@ -191,6 +191,13 @@ struct Handle {
   double *red = nullptr;      // partial sums workspace
   double *scal = nullptr;     // device scalars (errors, energies, means)
   double *hscal = nullptr;    // pinned host mirror of scal
+  // checkpoint snapshot (he4_snapshot_begin / he4_snapshot_wait): device
+  // copy of psi, rimp, vimp, aimp, its pinned host mirror, the copy stream
+  double *snap_dev = nullptr;
+  double *snap_host = nullptr;
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+  int snap_pending = 0;
   // radial histogram of the spherical bubble radius (grown on demand)
   unsigned long long *bub = nullptr;
   size_t bub_len = 0;

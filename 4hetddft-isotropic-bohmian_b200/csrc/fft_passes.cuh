@@ -488,16 +488,17 @@ __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
   const C2 *in = a.cin[blockIdx.y];
   TO *out = static_cast<TO *>(a.rout[blockIdx.y]);
   C2 *Sp = S + p * SP;
-  for (int k = j1; k < a.nxh; k += N1) {
-    C2 X = ina ? in[ra * a.nxh + k] : regfft::mk<C2>(0, 0);
-    C2 Y = inb ? in[rb * a.nxh + k] : regfft::mk<C2>(0, 0);
+  // the Hermitian extension of one row pair into S: X = row a, Y = row b
+  auto put = [&](int k, C2 X, C2 Y) {
     if (k == 0 || 2 * k == N) {  // DC / Nyquist of a real transform: drop Im
       X.y = 0;
       Y.y = 0;
     }
     Sp[k] = regfft::mk<C2>(X.x - Y.y, X.y + Y.x);
     if (k > 0 && N - k >= a.nxh) Sp[N - k] = regfft::mk<C2>(X.x + Y.y, Y.x - X.y);
-  }
+  };
+  for (int k = j1; k < a.nxh; k += N1)
+    put(k, ina ? in[ra * a.nxh + k] : regfft::mk<C2>(0, 0), inb ? in[rb * a.nxh + k] : regfft::mk<C2>(0, 0));
   __syncthreads();
   C2 v[N2];
 #pragma unroll

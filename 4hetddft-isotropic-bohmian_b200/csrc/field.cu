@@ -28,7 +28,8 @@ __global__ void k_grad(const double *__restrict__ f, double *dx, double *dy, dou
 // plane's tile with its periodic halo (about 2 loads per point instead of
 // 4M).  Every tap is summed in the order of stencil_axis, so the results are
 // those of the one-plane kernels.
-constexpr int kZB = 8;
+constexpr int kZB = 8;   // z extent the tile indices are checked for
+constexpr int kZBg = 4;  // planes per CTA of the gradient stencil
 
 struct OtArgs {
   double cp4, cpp4, den0s, h2o2m4, alphas, c_solid, beta, den_m;
@@ -77,14 +78,40 @@ __global__ void __launch_bounds__(256) k_grad_z(const double *__restrict__ f, TO
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 8, k0 = blockIdx.z * ZB;
   const int i = i0 + tx, j = j0 + ty;
   const bool in = i < g.nx && j < g.ny;
-  double q[ZB + 2 * M];
-  if (in) load_column<M, ZB>(f, g, i, j, k0, q);
+  const size_t ps = (size_t)g.ny * g.nx;
+  const int gi = wrap2(i, g.nx), gj = wrap2(j, g.ny);
+  // every global load of the ZB planes up front: the z column (queue), the
+  // x halo (threads tx < M) and the y halo (threads ty < M) of each plane;
+  // the planes then only wait for shared memory
+  double q[ZB + 2 * M], xl[ZB], xr[ZB], yl[ZB], yr[ZB];
+  load_column<M, ZB>(f, g, gi, gj, k0, q);
+#pragma unroll
+  for (int zz = 0; zz < ZB; zz++) {
+    const double *plane = f + (size_t)wrap2(k0 + zz, g.nz) * ps;
+    xl[zz] = xr[zz] = yl[zz] = yr[zz] = 0.0;
+    if (tx < M) {
+      xl[zz] = __ldg(plane + (size_t)gj * g.nx + wrap2(i0 - M + tx, g.nx));
+      xr[zz] = __ldg(plane + (size_t)gj * g.nx + wrap2(i0 + 32 + tx, g.nx));
+    }
+    if (ty < M) {
+      yl[zz] = __ldg(plane + (size_t)wrap2(j0 - M + ty, g.ny) * g.nx + gi);
+      yr[zz] = __ldg(plane + (size_t)wrap2(j0 + 8 + ty, g.ny) * g.nx + gi);
+    }
+  }
 #pragma unroll
   for (int zz = 0; zz < ZB; zz++) {
     const int k = k0 + zz;
     if (k >= g.nz) break;
     __syncthreads();
-    fill_tile<M, M>(f, g, i0, j0, k, in, in ? q[zz + M] : 0.0, s);
+    s[ty + M][tx + M] = q[zz + M];
+    if (tx < M) {
+      s[ty + M][tx] = xl[zz];
+      s[ty + M][tx + 32 + M] = xr[zz];
+    }
+    if (ty < M) {
+      s[ty][tx + M] = yl[zz];
+      s[ty + 8 + M][tx + M] = yr[zz];
+    }
     __syncthreads();
     if (!in) continue;
     double ax = 0.0, ay = 0.0, az = 0.0;
@@ -121,6 +148,25 @@ __global__ void __launch_bounds__(256) k_pot4_merged_z(const TI *__restrict__ li
   const bool in = i < g.nx && j < g.ny;
   const size_t ps = (size_t)g.ny * g.nx;
   double q[ZB + 2 * M], c0[ZB], c1[ZB], ld[ZB], dd[ZB], dcg[ZB];
+  // tile halos of every plane, loaded with the rest (threads tx < M: the x
+  // halo of h0; threads ty < M: the y halo of h1)
+  TI xl[ZB], xr[ZB], yl[ZB], yr[ZB];
+  const int gi = wrap2(i, g.nx), gj = wrap2(j, g.ny);
+  if (OTC) {
+#pragma unroll
+    for (int zz = 0; zz < ZB; zz++) {
+      const size_t pl = (size_t)wrap2(k0 + zz, g.nz) * ps;
+      xl[zz] = xr[zz] = yl[zz] = yr[zz] = TI(0);
+      if (tx < M) {
+        xl[zz] = __ldg(h0 + pl + (size_t)gj * g.nx + wrap2(i0 - M + tx, g.nx));
+        xr[zz] = __ldg(h0 + pl + (size_t)gj * g.nx + wrap2(i0 + 32 + tx, g.nx));
+      }
+      if (ty < M) {
+        yl[zz] = __ldg(h1 + pl + (size_t)wrap2(j0 - M + ty, g.ny) * g.nx + gi);
+        yr[zz] = __ldg(h1 + pl + (size_t)wrap2(j0 + 8 + ty, g.ny) * g.nx + gi);
+      }
+    }
+  }
   if (in) {
     if (OTC) load_column<M, ZB>(h2, g, i, j, k0, q);
 #pragma unroll
@@ -142,8 +188,17 @@ __global__ void __launch_bounds__(256) k_pot4_merged_z(const TI *__restrict__ li
     if (k >= g.nz) break;
     if (OTC) {
       __syncthreads();
-      fill_tile<M, 0>(h0, g, i0, j0, k, in, in ? c0[zz] : 0.0, s0);
-      fill_tile<0, M>(h1, g, i0, j0, k, in, in ? c1[zz] : 0.0, s1);
+      const size_t pl = (size_t)k * ps + (size_t)gj * g.nx + gi;
+      s0[ty][tx + M] = in ? c0[zz] : (double)__ldg(h0 + pl);
+      s1[ty + M][tx] = in ? c1[zz] : (double)__ldg(h1 + pl);
+      if (tx < M) {
+        s0[ty][tx] = (double)xl[zz];
+        s0[ty][tx + 32 + M] = (double)xr[zz];
+      }
+      if (ty < M) {
+        s1[ty][tx] = (double)yl[zz];
+        s1[ty + 8 + M][tx] = (double)yr[zz];
+      }
       __syncthreads();
     }
     if (!in) continue;
@@ -341,9 +396,9 @@ int launch_grad(Handle *h) {
   if (!zmarch_ok(h))
     k_grad<<<grid3(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
   else if (h->st.m == 3)
-    k_grad_z<3, kZB><<<grid_z(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+    k_grad_z<3, kZBg><<<grid_z(g, kZBg), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
   else
-    k_grad_z<6, kZB><<<grid_z(g), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
+    k_grad_z<6, kZBg><<<grid_z(g, kZBg), block3(), 0, h->stream>>>(h->den, h->dxden, h->dyden, h->dzden, h->st, g);
   HE4_LAUNCHED(h);
   return HE4_OK;
 }
@@ -516,9 +571,9 @@ static int field_poten_merged_f32(Handle *h) {
     HE4_TRY(fft_c2r_f32(h, otc ? 2 : 1, sp, out));
   }
   if (h->st.m == 3)
-    k_grad_z<3, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
+    k_grad_z<3, kZBg, float><<<grid_z(g, kZBg), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
   else
-    k_grad_z<6, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
+    k_grad_z<6, kZBg, float><<<grid_z(g, kZBg), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
   HE4_LAUNCHED(h);
   {
     const void *in[1] = {h->den};

@@ -24,6 +24,7 @@
 #include <iostream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/he4_tddft.h"
@@ -237,6 +238,51 @@ void printoutc(he4_handle *h, Run &r, double time, int iprint, const std::string
   he4io::write_impurity(f1, info, r.grid, r.psi, r.npar, r.rimp, r.vimp);
 }
 
+// printoutc backups every pcurr steps (DFT4He3d.f90:992-1009) without
+// stopping the time loop: the library snapshots the state and copies it to
+// pinned host memory while the next step runs; the files are then written
+// by a writer thread while the loop goes on.
+struct Backup {
+  bool pending = false;  // snapshot in flight, not yet collected
+  int iter = 0;
+  double time = 0.0;
+  std::string f, f1;
+  std::thread writer;
+};
+
+void backup_begin(he4_handle *h, Backup &b, double time, int iter, const std::string &f, const std::string &f1) {
+  if (b.writer.joinable()) b.writer.join();  // the pinned copy is reused
+  check(he4_snapshot_begin(h), "he4_snapshot_begin");
+  b.pending = true;
+  b.iter = iter;
+  b.time = time;
+  b.f = f;
+  b.f1 = f1;
+}
+
+void backup_collect(he4_handle *h, Run &r, Backup &b) {
+  if (!b.pending) return;
+  const double *psi = nullptr, *rimp = nullptr, *vimp = nullptr;
+  check(he4_snapshot_wait(h, &psi, &rimp, &vimp, nullptr), "he4_snapshot_wait");
+  b.pending = false;
+  he4io::PrintInfo info;
+  info.time = b.time;
+  info.iprint = r.binary ? -3 : 3;
+  info.iter = b.iter;
+  info.paflv = r.deltatps;
+  const size_t N = (size_t)r.p.nx * r.p.ny * r.p.nz, P3 = 3 * (size_t)r.npar;
+  const he4io::GridHeader grid = r.grid;
+  const int npar = r.npar;
+  const std::string f = b.f, f1 = b.f1;
+  b.writer = std::thread([=]() {
+    std::vector<std::complex<double>> ps(reinterpret_cast<const std::complex<double> *>(psi),
+                                         reinterpret_cast<const std::complex<double> *>(psi) + N);
+    std::vector<double> ri(rimp, rimp + P3), vi(vimp, vimp + P3);
+    he4io::write_psi(f, info, grid, ps);
+    he4io::write_impurity(f1, info, grid, ps, npar, ri, vi);
+  });
+}
+
 void denx_cuts(he4_handle *h, const Run &r, const double means[9]) {
   const size_t N = (size_t)r.p.nx * r.p.ny * r.p.nz;
   std::vector<double> denx(N);
@@ -374,6 +420,7 @@ int main(int argc, char **argv) {
   double eold = e.etot;
   // the time loop (DFT4He3d.f90:848-1045)
   const int first = r.iter0 + 1;
+  Backup bk;
   int iter = first;
   double time = r.time0;
   for (; iter <= r.niter; iter++) {
@@ -406,12 +453,16 @@ int main(int argc, char **argv) {
       bubble_block(h, r, f62, time);
       fflush(stdout);
     }
+    // the snapshot taken one step ago has reached host memory: write it
+    if (bk.pending && iter > bk.iter) backup_collect(h, r, bk);
     if (r.pcurr > 0 && iter % r.pcurr == 0) {
       const int ncurr = (iter - first + 1) / r.pcurr + r.icurr;
       const std::string tag = three_digits(ncurr);
-      printoutc(h, r, time, 3, "density." + tag + ".dat", "densityx." + tag + ".dat", iter);
+      backup_begin(h, bk, time, iter, "density." + tag + ".dat", "densityx." + tag + ".dat");
     }
   }
+  backup_collect(h, r, bk);
+  if (bk.writer.joinable()) bk.writer.join();
   fclose(f81);
   fclose(f82);
   fclose(f83);

@@ -205,6 +205,21 @@ int he4_diagnostics_noalloc(const double *den, int32_t nx, int32_t ny, int32_t n
                             double xmax, double ymax, double zmax, int32_t n4,
                             double *out, void *stream);
 
+/* Checkpoint without stopping the time loop (printoutc every pcurr steps,
+ * DFT4He3d.f90:992-1009, printoutc.f90:67-76).  he4_snapshot_begin copies
+ * psi, rimp, vimp and aimp into a device snapshot on the handle's stream and
+ * returns at once; the snapshot then travels to pinned host memory owned by
+ * the handle on a separate copy stream, overlapping the steps called next.
+ * he4_snapshot_wait waits for that copy and returns pointers into the
+ * pinned memory (psi [nz][ny][nx] complex as 2N doubles, the particle
+ * arrays [3][n_par]), valid until the next he4_snapshot_begin or
+ * he4_destroy.  One snapshot is in flight at a time: a second begin waits
+ * for the first copy.  The first call allocates the snapshot (16N + 72 n_par
+ * bytes on the device and as much pinned host memory). */
+int he4_snapshot_begin(he4_handle *h);
+int he4_snapshot_wait(he4_handle *h, const double **psi, const double **rimp,
+                      const double **vimp, const double **aimp);
+
 /* Copy-out of a real grid field ([nz][ny][nx]) or a half-spectrum kernel. */
 int he4_get_field(he4_handle *h, int32_t which, double *out);
 int he4_get_kernel(he4_handle *h, int32_t which, double *out);

@@ -67,8 +67,13 @@ def test_driver_run_matches_library(pkg, tmp_path):
                 g.steppc(dt)
             if it % 5 == 0:
                 e = g.energy()  # the driver prints these (iterations 5 and 10)
+            if it == 10:
+                at10 = g.get_state()[0]
         want = g.get_state()[0]
     assert np.array_equal(got, want)
+    # the pcurr backup (snapshot copied while the loop went on) holds the
+    # state of iteration 10
+    assert np.array_equal(read_psi(os.path.join(d, "density.001.dat"), psi.shape), at10)
     last_tot = [l for l in out.splitlines() if "TOTAL energy" in l][-1]
     assert float(last_tot.split()[-2]) == pytest.approx(e["etot"], abs=2e-6)
 
