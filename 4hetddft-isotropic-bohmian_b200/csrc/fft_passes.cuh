@@ -146,46 +146,8 @@ inline size_t smem_zconv() {
          (sizeof(long) + 2 * sizeof(int)) * W;
 }
 
-// in-place transform of strided pencils (y pass, or z without multiply)
-template <int N, int N1, bool INV, typename C2>
-__global__ void __launch_bounds__(kRegThreads) k_yz_reg(YRegArgs<C2> a) {
-  constexpr int N2 = N / N1, W = kRegThreads / N1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2 *S = reinterpret_cast<C2 *>(smem_raw), *tw = S + N * W;
-  long *offs = reinterpret_cast<long *>(tw + N);
-  load_tw_n<N>(tw, a.tw);
-  __shared__ int any;
-  if (threadIdx.x == 0) any = 0;
-  __syncthreads();
-  if (threadIdx.x < W) {
-    int kx, o;
-    long of = pencil_offset(a.map, (long)blockIdx.x * W + threadIdx.x, &kx, &o);
-    if (a.box && of >= 0) {  // pencils along y at plane z = o
-      int lo, hi;
-      force_range(a.box, 2, a.nz, &lo, &hi);
-      if (o < lo || o > hi) of = -1;
-    }
-    offs[threadIdx.x] = of;
-    if (of >= 0) any = 1;
-  }
-  __syncthreads();
-  if (!any) return;
-  const int w = threadIdx.x % W, j1 = threadIdx.x / W;
-  const long off = offs[w];
-  C2 *data = a.buf[blockIdx.y];
-  C2 v[N2];
-#pragma unroll
-  for (int j2 = 0; j2 < N2; j2++) v[j2] = (off >= 0) ? data[off + (j1 + N1 * j2) * a.sf] : regfft::mk<C2>(0, 0);
-  regfft::LayoutYZ lay{W, w};
-  regfft::fwd2<N, N1, INV>(v, S, lay, j1, tw);
-  if (off < 0) return;
-#pragma unroll
-  for (int c = 0; c < N2 / N1; c++)
-#pragma unroll
-    for (int k1 = 0; k1 < N1; k1++) data[off + ((j1 + N1 * c) + N2 * k1) * a.sf] = v[c * N1 + k1];
-}
-
-// Persistent, software-pipelined form of k_yz_reg: each CTA walks the
+// In-place transform of strided pencils (y pass, or z without multiply),
+// persistent and software-pipelined: each CTA walks the
 // pencil tiles blockIdx.x, blockIdx.x + gridDim.x, ... and loads the next
 // tile's values into registers before transforming the current one, so the
 // next tile's loads are in flight during the current tile's FFT and stores.
@@ -610,10 +572,6 @@ template <int N, int N1, typename C2>
 inline int reg_attrs() {
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_zsum_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_zsum<N, N1, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_yz_reg<N, N1, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_reg<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_yz_reg<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_pipe<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_yz_reg<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_yz_pipe<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -622,8 +580,6 @@ inline int reg_attrs() {
                                     (int)smem_zpipe<N, N1, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_pipe<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_zpipe<N, N1, C2>()));
-  HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, true, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_zconv<N, N1, true, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_zconv_reg<N, N1, false, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_zconv<N, N1, false, C2>()));
   HE4_CUDA_TRY(cudaFuncSetAttribute(k_xr2c_reg<N, N1, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
