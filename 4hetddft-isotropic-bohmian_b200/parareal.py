@@ -300,8 +300,9 @@ class Parareal:
         left, so the fallback starts right away.  judge_first (with fallback):
         the first iteration integrates slice 0 alone and compares its end with
         the coarse prediction before integrating slices 1.. from predicted
-        states; a rejected coarse step then costs no speculative fine sweep
-        and the run is the sequential integration plus the coarse sweep.
+        states; the coarse predictions of slices 1.. are made only once the
+        judge accepts, so a rejected coarse step costs one coarse step and no
+        speculative fine sweep: the run is the sequential integration.
         judge_max is the largest accepted coarse error over that slice; its
         default is tol, because the slices share one GPU here: a second
         iteration would already cost more fine steps than the sequential
@@ -318,8 +319,10 @@ class Parareal:
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record()
-        # initial coarse sweep
-        for n in range(self.S):
+        # initial coarse sweep; with the judge first, only the prediction of
+        # slice 0 is needed before the judge, the rest only if it accepts
+        lazy = judge_first and fallback and self.S > 1
+        for n in range(1 if lazy else self.S):
             self.G(self.U[n], self.U[n + 1])
             self.Gold[n + 1].copy_(self.U[n + 1])
         history = []
@@ -341,6 +344,9 @@ class Parareal:
                         fallback_at = 1
                         self._sequential(1, resume=True)
                         break
+                    for n in range(1, self.S):  # the rest of the coarse sweep
+                        self.G(self.U[n], self.U[n + 1])
+                        self.Gold[n + 1].copy_(self.U[n + 1])
                     self._fine(list(range(1, self.S)))
                 else:
                     self._fine(list(range(k - 1, self.S)))

@@ -99,9 +99,21 @@ def test_parareal_converges_to_sequential(pkg, setup):
         par.close()
 
 
+class Counting:
+    """A coarse propagator that counts its calls."""
+
+    def __init__(self, G):
+        self.G, self.calls = G, 0
+
+    def __call__(self, src, dst):
+        self.calls += 1
+        return self.G(src, dst)
+
+
 def test_parareal_fallback_is_the_sequential_solution(pkg, setup):
     s = setup
-    par = pkg.parareal.Parareal(s["p"], SLICES, STEPS, s["dt"], pkg.parareal.IdentityCoarse(STEPS * s["dt"]))
+    G = Counting(pkg.parareal.IdentityCoarse(STEPS * s["dt"]))
+    par = pkg.parareal.Parareal(s["p"], SLICES, STEPS, s["dt"], G)
     try:
         res = par.run(s["psi"], s["r"], s["v"], tol=1e-6)
         print("Morse impurity, G = identity:", res)
@@ -110,6 +122,7 @@ def test_parareal_fallback_is_the_sequential_solution(pkg, setup):
         # speculative sweep, every fine step is one of the sequential run,
         # which continues slice 0's integration (histories kept)
         assert res["fallback_at"] == 1 and res["fine_steps"] == SLICES * STEPS
+        assert G.calls == 1  # only slice 0's prediction was needed to judge it
         for n in range(1, SLICES + 1):
             assert rel(boundary_psi(par, n), s["ref_cont"][n - 1]) < 1e-12
     finally:
