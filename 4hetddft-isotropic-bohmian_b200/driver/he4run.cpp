@@ -177,7 +177,9 @@ void load_input(Run &r, const std::string &text) {
   } else if (selec == "null") {
     p.pot_kind = HE4_POT_NULL;
   } else {
-    die("Select_Pot entry '" + selec + "' is not built into the library: tabulate its Vq and give vqfile");
+    die("Select_Pot entry '" + selec +
+        "' is not built into the library: sample its V(r) from r_cutoff_gs on into vrfile, or tabulate its Vq "
+        "into vqfile");
   }
   r.n4 = (int)nl.integer("n4", 300);
   r.niter = (int)nl.integer("niter", 0);
@@ -377,6 +379,8 @@ int main(int argc, char **argv) {
            p.precision);
     printf("deltat=%.17g deltatps=%.17g niter=%d pener=%d pcurr=%d\n", r.deltat, r.deltatps, r.niter, r.pener,
            r.pcurr);
+    printf("n_vr=%d vr_r0=%.17g vr_dr=%.17g lbubble=%d lspherical=%d nr=%d\n", p.n_vr, p.vr_r0, p.vr_dr,
+           (int)r.lbubble, (int)r.lspherical, r.nr);
     double s = 0;
     for (const auto &c : r.psi) s += std::norm(c);
     printf("psi_norm2=%.17g rimp0=%.17g vimp_last=%.17g\n", s, r.rimp[0], r.vimp.back());

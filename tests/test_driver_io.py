@@ -138,4 +138,21 @@ def test_namelist_and_readenc(he4run, tmp_path):
     # unsupported Select_Pot entries ask for a table
     bad = nml.replace("selec_gs='morse'", "selec_gs='Ba_plus'")
     r = subprocess.run([he4run, "--print-input"], input=bad, capture_output=True, text=True)
-    assert r.returncode != 0 and "vqfile" in r.stderr
+    assert r.returncode != 0 and "vqfile" in r.stderr and "vrfile" in r.stderr
+    # any entry sampled on a uniform r grid (HE4_POT_RTABLE), and the
+    # spherical-bubble keys of the pener block
+    vr = tmp_path / "vr.dat"
+    rr = 3.0 + 0.01 * np.arange(500)
+    vr.write_text("".join(f" {a:.17E} {b:.17E}\n" for a, b in zip(rr, 10.0 * np.exp(-rr))))
+    good = nml.replace("selec_gs='morse',", f"selec_gs='He2S_fci', vrfile='{vr}',").replace(
+        "lbubble_radius=.false.", "lbubble_radius=.true., nr=301")
+    r = subprocess.run([he4run, "--print-input"], input=good, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    kv = dict(t.split("=") for t in r.stdout.split())
+    assert kv["pot_kind"] == "3" and kv["n_vr"] == "500"
+    assert float(kv["vr_r0"]) == 3.0 and float(kv["vr_dr"]) == pytest.approx(0.01, rel=1e-12)
+    assert kv["lbubble"] == "1" and kv["lspherical"] == "1" and kv["nr"] == "301"
+    # a table whose r values are not evenly spaced is refused
+    vr.write_text(" 3.0 1.0\n 3.1 0.5\n 3.3 0.2\n 3.4 0.1\n")
+    r = subprocess.run([he4run, "--print-input"], input=good, capture_output=True, text=True)
+    assert r.returncode != 0 and "uniformly" in r.stderr
