@@ -47,8 +47,8 @@ static int check_params(const he4_params *p) {
     set_error("npd=%d exceeds a grid dimension", p->npd);
     return HE4_E_ARG;
   }
-  if (p->icon != 8) {
-    set_error("icon=%d: only periodic boundary conditions (icon=8) are implemented", p->icon);
+  if (p->icon != 8 && p->icon != 13) {
+    set_error("icon=%d: only periodic (icon=8) and zero-padded (icon=13) boundaries are implemented", p->icon);
     return HE4_E_UNSUPPORTED;
   }
   if (p->core4 != HE4_CORE_OT && p->core4 != HE4_CORE_OTC) {

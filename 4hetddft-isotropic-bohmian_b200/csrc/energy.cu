@@ -61,7 +61,7 @@ __global__ void k_sumsq(const double *__restrict__ x, int n, double *out) {
 }
 
 int compute_energy(Handle *h, he4_energies *E) {
-  const Geo g{h->nx, h->ny, h->nz};
+  const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
   const he4_params &p = h->p;
   EArgs a;
   a.aux1 = 0.5 * p.cp4;

@@ -11,7 +11,7 @@
 
 namespace he4 {
 
-static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz}; }
+static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0}; }
 
 // derden (derden.f90:26-28)
 __global__ void k_grad(const double *__restrict__ f, double *dx, double *dy, double *dz, Stencil st, Geo g) {
@@ -423,7 +423,8 @@ __global__ void k_gather(const double *__restrict__ rimp, const double *__restri
 // nx >= 40, ny >= 16 and nz >= kZB + 2m: the farthest halo cell lies at most
 // 36 cells beyond the last x index and 12 beyond the last y and z index.
 static bool zmarch_ok(const Handle *h) {
-  return (h->st.m == 3 || h->st.m == 6) && h->nx >= 40 && h->ny >= 16 && h->nz >= kZB + 2 * h->st.m;
+  return h->p.icon == 8 && (h->st.m == 3 || h->st.m == 6) && h->nx >= 40 && h->ny >= 16 &&
+         h->nz >= kZB + 2 * h->st.m;
 }
 
 static dim3 grid_z(const Geo &g, int zb = kZB) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + zb - 1) / zb); }
@@ -766,10 +767,22 @@ int field_forces(Handle *h, bool full) {
   // (potenimp.f90:42-50, with the 1/m_X of :67-69 folded in)
   const double c = -h->renor / h->mAg_u;
   const int bz = full ? 0 : 1;
-  ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, c, 0, 0, bz},
-                {h->spec[0], h->spec[2], h->vq, c, 1, 0, bz},
-                {h->spec[0], h->spec[3], h->vq, c, 2, 0, bz}};
-  HE4_TRY(fft_z_conv(h, 3, ops));
+  if (h->p.icon == 8) {
+    ZOp ops[3] = {{h->spec[0], h->spec[1], h->vq, c, 0, 0, bz},
+                  {h->spec[0], h->spec[2], h->vq, c, 1, 0, bz},
+                  {h->spec[0], h->spec[3], h->vq, c, 2, 0, bz}};
+    HE4_TRY(fft_z_conv(h, 3, ops));
+  } else {
+    // non-periodic stencils: FFT(d_i rho) is no multiple of FFT(rho), so the
+    // gradients of this evaluation are transformed as the reference does
+    const double *in[3] = {h->dxden, h->dyden, h->dzden};
+    double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
+    HE4_TRY(fft_r2c(h, 3, in, sp));
+    ZOp ops[3] = {{h->spec[1], h->spec[1], h->vq, c, -1, 0, bz},
+                  {h->spec[2], h->spec[2], h->vq, c, -1, 0, bz},
+                  {h->spec[3], h->spec[3], h->vq, c, -1, 0, bz}};
+    HE4_TRY(fft_z_conv(h, 3, ops));
+  }
   double2 *sp[3] = {h->spec[1], h->spec[2], h->spec[3]};
   double *out[3] = {h->fx, h->fy, h->fz};
   if (full)

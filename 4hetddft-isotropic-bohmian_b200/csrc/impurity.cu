@@ -240,7 +240,7 @@ static unsigned box_grid(const Handle *h) {
 }
 
 int impurity_density(Handle *h) {
-  const Geo g{h->nx, h->ny, h->nz};
+  const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
   const DepArgs d = dep_args(h);
   const unsigned gb = box_grid(h);
   k_box_find<<<1, 1024, 0, h->stream>>>(h->rimp, d, h->p.ironx, h->st.m, h->box);
@@ -266,7 +266,7 @@ int impurity_density(Handle *h) {
 }
 
 int impurity_force_q(Handle *h) {
-  const Geo g{h->nx, h->ny, h->nz};
+  const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
   k_force_q_box<<<box_grid(h), 256, 0, h->stream>>>(h->box, h->fx, h->fy, h->fz, h->psix, h->hpsix, h->denx,
                                                    h->mAg_u, h->st, g);
   HE4_LAUNCHED(h);

@@ -1,8 +1,11 @@
-// stencil.cuh -- periodic npd-point finite differences on the device.
+// stencil.cuh -- npd-point finite differences on the device.
 //
-// Restates Deriv3D_p / Deriv3D_pc for icon=8 (init_deriv_parallel.f90:
-// 1100-1205, 475-650): df(i) = sum_{t=-m..m} Cd(ko2p1, t) f(i+t) with indices
-// wrapped periodically, Cd = centre row of the Bickley matrix times 1/h^id.
+// Restates Deriv3D_p / Deriv3D_pc (init_deriv_parallel.f90:1100-1205,
+// 475-650): df(i) = sum_{t=-m..m} Cd(ko2p1, t) f(i+t), Cd = centre row of the
+// Bickley matrix times 1/h^id.  icon=8: indices wrap periodically.  icon=13:
+// Redef (redef.f:133-170) makes each of the ko2 boundary rows at either end
+// the centre row shifted by one more place, its taps past the end dropped,
+// which is the same sum with f = 0 outside the grid (Geo::zpad).
 #pragma once
 #include "common.cuh"
 
@@ -10,14 +13,25 @@ namespace he4 {
 
 struct Geo {
   int nx, ny, nz;
+  int zpad = 0;  // icon=13: taps outside the grid are dropped instead of wrapped
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// sum_t w[t] * f(i + t e_axis), periodic; sequential order t = -m..m
-__device__ __forceinline__ double stencil_axis(const double *__restrict__ f, const double *w, int m, const Geo &g,
-                                               int i, int j, int k, int axis) {
+// sum_t w[t] * f(i + t e_axis), sequential order t = -m..m; ZPAD: taps
+// outside the grid dropped (icon=13), else indices wrapped (icon=8)
+template <bool ZPAD>
+__device__ __forceinline__ double stencil_axis_t(const double *__restrict__ f, const double *w, int m, const Geo &g,
+                                                 int i, int j, int k, int axis) {
   double acc = 0.0;
+  if constexpr (ZPAD) {
+    const int c = (axis == 0) ? i : (axis == 1) ? j : k, n = (axis == 0) ? g.nx : (axis == 1) ? g.ny : g.nz;
+    const size_t st = (axis == 0) ? 1 : (axis == 1) ? (size_t)g.nx : (size_t)g.nx * g.ny;
+    const double *p0 = f + ((size_t)k * g.ny + j) * g.nx + i;
+    for (int t = -m; t <= m; t++)
+      if (c + t >= 0 && c + t < n) acc += w[t + m] * __ldg(p0 + (long)t * (long)st);
+    return acc;
+  }
   if (axis == 0) {
     const double *row = f + ((size_t)k * g.ny + j) * g.nx;
     for (int t = -m; t <= m; t++) acc += w[t + m] * __ldg(row + wrap(i + t, g.nx));
@@ -32,9 +46,28 @@ __device__ __forceinline__ double stencil_axis(const double *__restrict__ f, con
   return acc;
 }
 
-__device__ __forceinline__ double2 stencil_axis_c(const double2 *__restrict__ f, const double *w, int m,
-                                                  const Geo &g, int i, int j, int k, int axis) {
+// the periodic or zero-padded form as the grid says
+__device__ __forceinline__ double stencil_axis(const double *__restrict__ f, const double *w, int m, const Geo &g,
+                                               int i, int j, int k, int axis) {
+  return g.zpad ? stencil_axis_t<true>(f, w, m, g, i, j, k, axis) : stencil_axis_t<false>(f, w, m, g, i, j, k, axis);
+}
+
+template <bool ZPAD>
+__device__ __forceinline__ double2 stencil_axis_c_t(const double2 *__restrict__ f, const double *w, int m,
+                                                    const Geo &g, int i, int j, int k, int axis) {
   double ar = 0.0, ai = 0.0;
+  if constexpr (ZPAD) {
+    const int c = (axis == 0) ? i : (axis == 1) ? j : k, n = (axis == 0) ? g.nx : (axis == 1) ? g.ny : g.nz;
+    const size_t st = (axis == 0) ? 1 : (axis == 1) ? (size_t)g.nx : (size_t)g.nx * g.ny;
+    const double2 *p0 = f + ((size_t)k * g.ny + j) * g.nx + i;
+    for (int t = -m; t <= m; t++)
+      if (c + t >= 0 && c + t < n) {
+        const double2 v = __ldg(p0 + (long)t * (long)st);
+        ar += w[t + m] * v.x;
+        ai += w[t + m] * v.y;
+      }
+    return make_double2(ar, ai);
+  }
   if (axis == 0) {
     const double2 *row = f + ((size_t)k * g.ny + j) * g.nx;
     for (int t = -m; t <= m; t++) {
@@ -61,12 +94,19 @@ __device__ __forceinline__ double2 stencil_axis_c(const double2 *__restrict__ f,
   return make_double2(ar, ai);
 }
 
+__device__ __forceinline__ double2 stencil_axis_c(const double2 *__restrict__ f, const double *w, int m,
+                                                  const Geo &g, int i, int j, int k, int axis) {
+  return g.zpad ? stencil_axis_c_t<true>(f, w, m, g, i, j, k, axis)
+                : stencil_axis_c_t<false>(f, w, m, g, i, j, k, axis);
+}
+
 // complex Laplacian (sum of the three second derivatives, x + y + z)
-__device__ __forceinline__ double2 lap_c(const double2 *__restrict__ f, const Stencil &st, const Geo &g, int i,
-                                         int j, int k) {
-  double2 a = stencil_axis_c(f, st.w2[0], st.m, g, i, j, k, 0);
-  double2 b = stencil_axis_c(f, st.w2[1], st.m, g, i, j, k, 1);
-  double2 c = stencil_axis_c(f, st.w2[2], st.m, g, i, j, k, 2);
+template <bool ZPAD>
+__device__ __forceinline__ double2 lap_c_t(const double2 *__restrict__ f, const Stencil &st, const Geo &g, int i,
+                                           int j, int k) {
+  double2 a = stencil_axis_c_t<ZPAD>(f, st.w2[0], st.m, g, i, j, k, 0);
+  double2 b = stencil_axis_c_t<ZPAD>(f, st.w2[1], st.m, g, i, j, k, 1);
+  double2 c = stencil_axis_c_t<ZPAD>(f, st.w2[2], st.m, g, i, j, k, 2);
   return make_double2((a.x + b.x) + c.x, (a.y + b.y) + c.y);
 }
 

@@ -21,7 +21,7 @@
 
 namespace he4 {
 
-static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz}; }
+static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0}; }
 
 __global__ void k_finalize_sums(const double *__restrict__ part, size_t stride, int nb, int nvals, double mult,
                                 double div, double *out) {
@@ -39,11 +39,12 @@ struct PsiArgs {
   const double *timec_re;  // [nz]
 };
 
-// H psi (the Sto4c of steppc.f90:46 / steprk.f90:218)
+// H psi (the Sto4c of steppc.f90:46 / steprk.f90:218); ZPAD: icon=13
+template <bool ZPAD>
 __device__ __forceinline__ double2 hpsi_at(const double2 *__restrict__ psi, const double *__restrict__ pot4,
                                            const Stencil &st, const Geo &g, const PsiArgs &a, int i, int j, int k,
                                            size_t t) {
-  const double2 lap = lap_c(psi, st, g, i, j, k);
+  const double2 lap = lap_c_t<ZPAD>(psi, st, g, i, j, k);
   const double2 ps = psi[t];
   const double v = pot4[t];
   const double2 w = make_double2(lap.x * a.h2o2m4 - v * ps.x, lap.y * a.h2o2m4 - v * ps.y);
@@ -52,11 +53,12 @@ __device__ __forceinline__ double2 hpsi_at(const double2 *__restrict__ psi, cons
 }
 
 // one RK-Gill stage (steprk.f90:211-229)
+template <bool ZPAD>
 __global__ void k_rk_stage(const double2 *__restrict__ psi, const double *__restrict__ pot4, double2 *q,
                            double2 *psi_out, double *den, double2 *h_first, double2 *p_first, double ar, double br,
                            double cr, Stencil st, Geo g, PsiArgs a) {
   HE4_IJK(g);
-  const double2 s4 = hpsi_at(psi, pot4, st, g, a, i, j, k, t);
+  const double2 s4 = hpsi_at<ZPAD>(psi, pot4, st, g, a, i, j, k, t);
   const double2 qv = q[t];
   const double2 s1 = make_double2(ar * (s4.x - br * qv.x), ar * (s4.y - br * qv.y));
   q[t] = make_double2(qv.x + 3.0 * s1.x - cr * s4.x, qv.y + 3.0 * s1.y - cr * s4.y);
@@ -71,12 +73,13 @@ __global__ void k_rk_stage(const double2 *__restrict__ psi, const double *__rest
 }
 
 // predictor + modifier (steppc.f90:36-56)
+template <bool ZPAD>
 __global__ void k_pc_predict(const double2 *__restrict__ psi, const double *__restrict__ pot4, double2 *p3,
                              const double2 *__restrict__ h1, double2 *h2, double2 *pc, double *den, Stencil st, Geo g,
                              PsiArgs a) {
   HE4_IJK(g);
   const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
-  const double2 s4 = hpsi_at(psi, pot4, st, g, a, i, j, k, t);
+  const double2 s4 = hpsi_at<ZPAD>(psi, pot4, st, g, a, i, j, k, t);
   const double2 o3 = p3[t], f1 = h1[t], f2 = h2[t];
   const double f = c4o3 * a.dt;
   const double2 pr = make_double2(o3.x + f * (2.0 * s4.x - f1.x + 2.0 * f2.x),
@@ -91,6 +94,7 @@ __global__ void k_pc_predict(const double2 *__restrict__ psi, const double *__re
 
 // corrector + final value (steppc.f90:97-112); per-block partial sums of
 // |pc| for errHe
+template <bool ZPAD>
 __global__ void k_pc_correct(const double2 *__restrict__ psi, const double *__restrict__ pot4,
                              const double2 *__restrict__ p3, const double2 *__restrict__ p2,
                              const double2 *__restrict__ h1, const double2 *__restrict__ h2, double2 *pc,
@@ -103,7 +107,7 @@ __global__ void k_pc_correct(const double2 *__restrict__ psi, const double *__re
   if (i < g.nx && j < g.ny) {
     const size_t t = ((size_t)k * g.ny + j) * g.nx + i;
     const double c9 = 9.0 / 121.0;
-    const double2 s4 = hpsi_at(psi, pot4, st, g, a, i, j, k, t);
+    const double2 s4 = hpsi_at<ZPAD>(psi, pot4, st, g, a, i, j, k, t);
     const double2 o3 = p3[t], o2 = p2[t], f1 = h1[t], f2 = h2[t];
     const double d3 = 3.0 * a.dt;
     const double2 s5 = make_double2(0.125 * (9.0 * o3.x - o2.x + d3 * (s4.x + 2.0 * f1.x - f2.x)),
@@ -305,8 +309,12 @@ int step_rk(Handle *h, double dt, double *dres) {
       hf = h->hpsiold[0];
       pf = h->psiold[0];
     }
-    k_rk_stage<<<grid3(g), block3(), 0, h->stream>>>(h->psi, h->pot4, h->q, h->ctmp, h->den, hf, pf, arun[jr],
-                                                     brun[jr], crun[jr], h->st, g, pa);
+    if (g.zpad)
+      k_rk_stage<true><<<grid3(g), block3(), 0, h->stream>>>(h->psi, h->pot4, h->q, h->ctmp, h->den, hf, pf,
+                                                             arun[jr], brun[jr], crun[jr], h->st, g, pa);
+    else
+      k_rk_stage<false><<<grid3(g), block3(), 0, h->stream>>>(h->psi, h->pot4, h->q, h->ctmp, h->den, hf, pf,
+                                                              arun[jr], brun[jr], crun[jr], h->st, g, pa);
     HE4_LAUNCHED(h);
     std::swap(h->psi, h->ctmp);
     if (jr == 0) {
@@ -335,8 +343,12 @@ int step_pc(Handle *h, double dt, double *dres) {
   // predictor + modifier for psi
   {
     double2 *p3 = h->psiold[h->ioldp[2]];
-    k_pc_predict<<<grid3(g), block3(), 0, h->stream>>>(h->psi, h->pot4, p3, h->hpsiold[h->ioldh[0]],
-                                                       h->hpsiold[h->ioldh[1]], h->pc, h->den, h->st, g, pa);
+    if (g.zpad)
+      k_pc_predict<true><<<grid3(g), block3(), 0, h->stream>>>(h->psi, h->pot4, p3, h->hpsiold[h->ioldh[0]],
+                                                               h->hpsiold[h->ioldh[1]], h->pc, h->den, h->st, g, pa);
+    else
+      k_pc_predict<false><<<grid3(g), block3(), 0, h->stream>>>(h->psi, h->pot4, p3, h->hpsiold[h->ioldh[0]],
+                                                                h->hpsiold[h->ioldh[1]], h->pc, h->den, h->st, g, pa);
     HE4_LAUNCHED(h);
     std::swap(h->psi, h->psiold[h->ioldp[2]]);
     std::swap(h->ioldh[0], h->ioldh[1]);
@@ -350,9 +362,16 @@ int step_pc(Handle *h, double dt, double *dres) {
   {
     dim3 gr = grid3(g);
     const int nb = (int)(gr.x * gr.y * gr.z);
-    k_pc_correct<<<gr, block3(), 0, h->stream>>>(h->psi, h->pot4, h->psiold[h->ioldp[2]], h->psiold[h->ioldp[1]],
-                                                 h->hpsiold[h->ioldh[0]], h->hpsiold[h->ioldh[1]], h->pc, h->ctmp,
-                                                 h->den, h->red, h->st, g, pa);
+    if (g.zpad)
+      k_pc_correct<true><<<gr, block3(), 0, h->stream>>>(h->psi, h->pot4, h->psiold[h->ioldp[2]],
+                                                         h->psiold[h->ioldp[1]], h->hpsiold[h->ioldh[0]],
+                                                         h->hpsiold[h->ioldh[1]], h->pc, h->ctmp, h->den, h->red,
+                                                         h->st, g, pa);
+    else
+      k_pc_correct<false><<<gr, block3(), 0, h->stream>>>(h->psi, h->pot4, h->psiold[h->ioldp[2]],
+                                                          h->psiold[h->ioldp[1]], h->hpsiold[h->ioldh[0]],
+                                                          h->hpsiold[h->ioldh[1]], h->pc, h->ctmp, h->den, h->red,
+                                                          h->st, g, pa);
     HE4_LAUNCHED(h);
     std::swap(h->psi, h->ctmp);
     rot3(h->ioldp);

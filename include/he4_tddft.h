@@ -66,7 +66,8 @@ typedef struct he4_params {
   /* grid (namelist nx,ny,nz,xmax,ymax,zmax; DFT4He3d.f90:271-354) */
   int32_t nx, ny, nz;
   double xmax, ymax, zmax;
-  /* derivatives (module deriva): npd odd in [3,25]; icon 8 = periodic */
+  /* derivatives (module deriva): npd odd in [3,25]; icon 8 = periodic,
+   * icon 13 = centred stencils with f = 0 outside the grid (redef.f:133-170) */
   int32_t npd, icon;
   /* functional */
   int32_t core4;

@@ -796,7 +796,7 @@ int ora_create(const he4_params *pin, ora_state **out) {
   if (!pin || !out) return HE4_E_ARG;
   const he4_params *p = pin;
   if (!valid_n(p->nx) || !valid_n(p->ny) || !valid_n(p->nz)) return HE4_E_ARG;
-  if (p->icon != 8) return HE4_E_UNSUPPORTED;
+  if (p->icon != 8 && p->icon != 13) return HE4_E_UNSUPPORTED;
   if (p->npd < 3 || p->npd > 25 || p->npd % 2 == 0) return HE4_E_ARG;
   if (p->n_par < 1 || p->ironx < 0) return HE4_E_ARG;
   if (p->core4 != HE4_CORE_OT && p->core4 != HE4_CORE_OTC) return HE4_E_UNSUPPORTED;
@@ -955,14 +955,17 @@ void ora_destroy(ora_state *s) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* derivatives: periodic (icon=8) npd-point stencils, Deriv3D_p / Deriv3D_pc */
-/* (init_deriv_parallel.f90:373-655 and 938-1213, periodic branch)           */
+/* derivatives: npd-point stencils, Deriv3D_p / Deriv3D_pc                   */
+/* (init_deriv_parallel.f90:373-655 and 938-1213).  icon=8: periodic.       */
+/* icon=13: Redef (redef.f:133-170) replaces the ko2 boundary rows at each   */
+/* end by the centre row shifted one place per row, its taps past the end   */
+/* dropped, i.e. the centred stencil with f = 0 outside the grid.            */
 /* ------------------------------------------------------------------------ */
 
 static void deriv_r(const ora_state *s, int id, int axis, const double *f, double *df) {
   int nx = s->nx, ny = s->ny, nz = s->nz, m = s->p.npd / 2;
   const double *w = (id == 1) ? s->w1[axis] : s->w2[axis];
-  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz;
+  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz, zpad = (s->p.icon == 13);
   if (n < s->p.npd) { memset(df, 0, sizeof(double) * s->N); return; }
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < nz; k++)
@@ -971,6 +974,10 @@ static void deriv_r(const ora_state *s, int id, int axis, const double *f, doubl
         double acc = 0.0;
         for (int t = -m; t <= m; t++) {
           int ii = i, jj = j, kk = k;
+          if (zpad) {
+            int q = (axis == 0 ? i : axis == 1 ? j : k) + t;
+            if (q < 0 || q >= n) continue;
+          }
           if (axis == 0) ii = (i + t + nx) % nx;
           else if (axis == 1) jj = (j + t + ny) % ny;
           else kk = (k + t + nz) % nz;
@@ -983,7 +990,7 @@ static void deriv_r(const ora_state *s, int id, int axis, const double *f, doubl
 static void deriv_c(const ora_state *s, int id, int axis, const cplx *f, cplx *df) {
   int nx = s->nx, ny = s->ny, nz = s->nz, m = s->p.npd / 2;
   const double *w = (id == 1) ? s->w1[axis] : s->w2[axis];
-  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz;
+  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz, zpad = (s->p.icon == 13);
   if (n < s->p.npd) { memset(df, 0, sizeof(cplx) * s->N); return; }
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < nz; k++)
@@ -992,6 +999,10 @@ static void deriv_c(const ora_state *s, int id, int axis, const cplx *f, cplx *d
         double ar = 0.0, ai = 0.0;
         for (int t = -m; t <= m; t++) {
           int ii = i, jj = j, kk = k;
+          if (zpad) {
+            int q = (axis == 0 ? i : axis == 1 ? j : k) + t;
+            if (q < 0 || q >= n) continue;
+          }
           if (axis == 0) ii = (i + t + nx) % nx;
           else if (axis == 1) jj = (j + t + ny) % ny;
           else kk = (k + t + nz) % nz;

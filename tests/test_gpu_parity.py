@@ -124,6 +124,52 @@ def test_field_parity(pkg, c1):
             assert abs(eg[k] - eo[k]) <= 1e-10 * max(abs(eo[k]), 1e-30), (k, eg[k], eo[k])
 
 
+@pytest.fixture(scope="module")
+def c1_icon13(pkg, ora):
+    """64^3 with icon=13 (zero-padded stencils, the shipped inputs' mode) and a
+    droplet of 600 atoms (R = 18.7 A) whose density reaches the box faces, so
+    the boundary rows matter."""
+    w = pkg.workloads
+    p = w.make_params(64, 0.6, 256)
+    p.icon = 13
+    psi = w.droplet_psi(p, 600)
+    r, v = w.particles(256, 1234, 100.0)
+    o = ora.Oracle(p)
+    return p, psi, r, v, o, o.get_kernel("vq")
+
+
+def test_field_and_steps_parity_icon13(pkg, c1_icon13):
+    p, psi, r, v, o, vq = c1_icon13
+    o.set_state(psi, r, v)
+    o.field()
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        g.field()
+        for name in pkg.abi.FIELDS:
+            assert rel(g.get_field(name), o.get_field(name)) < 1e-11, name
+        assert rel(g.get_state()[3], o.get_state()[3]) < 1e-11
+        # the boundary mode is live: the periodic stencils give other fields
+        q = pkg.abi.He4Params.from_buffer_copy(p)
+        q.icon = 8
+        with gpu_with_table(pkg, q, vq) as g8:
+            g8.set_state(psi, r, v)
+            g8.field()
+            assert rel(g8.get_field("dxden"), g.get_field("dxden")) > 1e-6
+    dt = pkg.workloads.deltat_fs(1.0)
+    o.set_state(psi, r, v)
+    eo, mo = o.run(8, dt)
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        eg, mg = g.run(8, dt)
+        assert np.allclose(eg[3:], eo[3:], rtol=1e-8, atol=0)
+        assert np.allclose(mg, mo, rtol=1e-9, atol=1e-9 * np.abs(mo).max())
+        assert rel(g.get_field("pot4"), o.get_field("pot4")) < 1e-10
+        assert rel(g.get_state()[0], o.get_state()[0]) < 1e-10
+        Eg, Eo = g.energy(), o.energy()
+        for k in Eo:
+            assert abs(Eg[k] - Eo[k]) <= 1e-10 * max(abs(Eo[k]), 1e-30), (k, Eg[k], Eo[k])
+
+
 def test_steps_parity(pkg, c1):
     p, psi, r, v, o, vq = c1
     dt = pkg.workloads.deltat_fs(1.0)

@@ -209,6 +209,54 @@ def test_periodic_stencils_match_fourier_symbol(pkg, ora, small):
     _ = x
 
 
+def redef13_rows(c, n):
+    """Deriv3D_p's matrix for icon=13 built as Redef does it (redef.f:151-170
+    then :133-150): the ko2 rows before the centre row are the centre row
+    shifted left one place per row, the ko2 rows after it shifted right, the
+    vacated entry zero; row i < ko2 acts on f(1..k), row i > n-1-ko2 on
+    f(n-k+1..n), the rest is the centre row around i.  Returns the n x n
+    matrix of the derivative."""
+    k = len(c)
+    ko2 = k // 2
+    cd = np.zeros((k, k))
+    cd[ko2] = c
+    for i in range(ko2 - 1, -1, -1):  # rows KO2..1
+        cd[i, :k - 1] = cd[i + 1, 1:]
+        cd[i, k - 1] = 0.0
+    for i in range(ko2 + 1, k):  # rows KO2P2..K
+        cd[i, 1:] = cd[i - 1, :k - 1]
+        cd[i, 0] = 0.0
+    D = np.zeros((n, n))
+    for i in range(n):
+        if i < ko2:
+            D[i, :k] = cd[i]
+        elif i >= n - ko2:
+            D[i, n - k:] = cd[i - n + k]
+        else:
+            D[i, i - ko2:i + ko2 + 1] = c
+    return D
+
+
+@pytest.mark.parametrize("npd", [7, 13])
+def test_icon13_stencils_are_redef_rows(pkg, ora, npd):
+    """icon=13 (the shipped inputs' boundary mode): the oracle's derivatives
+    equal the matrix Redef builds, along each axis, for both orders."""
+    p = pkg.workloads.make_params(16, 0.6, 8, npd=npd, ny=20, nz=24)
+    p.icon = 13
+    o = ora.Oracle(p)
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((p.nz, p.ny, p.nx))
+    h = 2 * p.xmax / p.nx
+    for order in (1, 2):
+        c = np.asarray(ora.fd_weights(npd, order)) / h ** order
+        for axis, n in ((0, p.nx), (1, p.ny), (2, p.nz)):
+            D = redef13_rows(c, n)
+            want = np.moveaxis(np.tensordot(D, np.moveaxis(f, 2 - axis, 0), axes=(1, 0)), 0, 2 - axis)
+            got = o.deriv(f, order, axis)
+            assert np.allclose(got, want, rtol=1e-13, atol=1e-12 * np.max(np.abs(want))), (order, axis)
+    o.close()
+
+
 def test_field_consistency_free_droplet(pkg, ora):
     """Without particles near the grid the impurity terms vanish and the
     He mean field is symmetric under z -> -z for a centred droplet."""
