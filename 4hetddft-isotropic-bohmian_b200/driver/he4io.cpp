@@ -307,6 +307,19 @@ void read_psi(const std::string &path, GridHeader *h, std::vector<std::complex<d
   for (size_t k = 0; k < N; k++) (*psi)[k] = r.cplx();
 }
 
+void read_density(const std::string &path, GridHeader *h, std::vector<double> *den) {
+  const std::string s = slurp(path);
+  ListReader r(s, after_comments(s));
+  h->xmax = r.real(), h->ymax = r.real(), h->zmax = r.real();
+  h->hx = r.real(), h->hy = r.real(), h->hz = r.real();
+  h->nx = (int)r.integer(), h->ny = (int)r.integer(), h->nz = (int)r.integer();
+  r.raw();  // limp (logical)
+  r.real(), r.real(), r.real();  // ximp, yimp, zimp
+  const size_t N = (size_t)h->nx * h->ny * h->nz;
+  den->resize(N);
+  for (size_t k = 0; k < N; k++) (*den)[k] = r.real();
+}
+
 void read_impurity(const std::string &path, int *npar, std::vector<double> *rimp, std::vector<double> *vimp) {
   if (looks_binary(path, 4)) {
     FILE *f = fopen(path.c_str(), "rb");

@@ -1,5 +1,5 @@
 // he4io.hpp -- host-side input and output of the time-dependent run: the
-// &input namelist (DFT4He3d.f90:147-187), readenc mode 2 (readenc.f90:96-114,
+// &input namelist (DFT4He3d.f90:147-187), readenc modes 0 and 2 (readenc.f90:78-114,
 // with titols.f90's comment skipping) and printoutc (printoutc.f90:13-131),
 // formatted (Fortran list-directed) and binary (Fortran unformatted
 // sequential, 4-byte record markers).
@@ -41,6 +41,9 @@ struct GridHeader {
 // (printoutc with iprint < 0) are recognised by their first record marker.
 void read_psi(const std::string &path, GridHeader *hdr, std::vector<std::complex<double>> *psi);
 void read_impurity(const std::string &path, int *npar, std::vector<double> *rimp, std::vector<double> *vimp);
+// readenc mode 0 (readenc.f90:78-92): a real density file whose header line
+// holds xmax,ymax,zmax,hx,hy,hz,nx,ny,nz,limp,ximp,yimp,zimp, then den(nx,ny,nz).
+void read_density(const std::string &path, GridHeader *hdr, std::vector<double> *den);
 
 // printoutc: iprint 1 (last printout), 2 (Paflov change) or 3 (backup)
 // with the formatted header comments; iprint < 0 writes the binary form.

@@ -18,10 +18,12 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <fstream>
 #include <iostream>
+#include <random>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -98,6 +100,14 @@ struct Run {
   std::string file_spherical_bubble;
   double deltat = 0, deltatps = 0, time0 = 0;
   std::string filedenin, fileimpin, filedenout, fileimpout, filerimp, filevimp, fileaimp;
+  // readenc mode 0 start (DFT4He3d.f90:585-617): phase constraints, the box
+  // the particles are drawn in, their common velocity (A/ps), the seed of
+  // the draw (the reference's random_number is unseeded)
+  int mode = 0;
+  double xlamdax = 0, xlamday = 0, xlamdaz = 0;
+  double xi = 1e99, xf = 1e99, yi = 1e99, yf = 1e99, zi = 1e99, zf = 1e99;
+  double v0[3] = {0, 0, 0};
+  unsigned long long seed = 1;
 };
 
 void load_input(Run &r, const std::string &text) {
@@ -202,7 +212,22 @@ void load_input(Run &r, const std::string &text) {
   } else if (r.deltatps == 0.0) {
     r.deltatps = r.deltat * kKtops;
   }
-  if (nl.integer("mode", 2) != 2) die("only readenc mode 2 (wave function + impurity file) feeds the time step");
+  r.mode = (int)nl.integer("mode", 0);
+  if (r.mode != 0 && r.mode != 2) die("ERROR READEN: This mode is still not programmed");  // readenc.f90:116-121
+  r.xlamdax = nl.real("xlamdax", 0.0);
+  r.xlamday = nl.real("xlamday", 0.0);
+  r.xlamdaz = nl.real("xlamdaz", 0.0);
+  const double xlamda = nl.real("xlamda", 0.0);
+  if (xlamda != 0.0) r.xlamdaz = xlamda * kKtops / (2.0 * p.h2o2m4);  // DFT4He3d.f90:579-582
+  r.xi = nl.real("xi", 1e99), r.xf = nl.real("xf", 1e99);
+  r.yi = nl.real("yi", 1e99), r.yf = nl.real("yf", 1e99);
+  r.zi = nl.real("zi", 1e99), r.zf = nl.real("zf", 1e99);
+  r.v0[0] = nl.real("v0x", 0.0), r.v0[1] = nl.real("v0y", 0.0), r.v0[2] = nl.real("v0z", 0.0);
+  r.seed = (unsigned long long)nl.integer("seed", 1);
+  // the reference asks for the particle box at every start (DFT4He3d.f90:188-196);
+  // only the mode-0 draw uses it here
+  if (r.mode == 0 && (r.xi > 1e10 || r.xf > 1e10 || r.yi > 1e10 || r.yf > 1e10 || r.zi > 1e10 || r.zf > 1e10))
+    die("Has de definirme los limites de la impuerza... (xi, xf, yi, yf, zi, zf)");
   r.filedenin = nl.str("filedenin", "he4.input.density");
   r.fileimpin = nl.str("fileimpin", "X.input.wf");
   r.filedenout = nl.str("filedenout", "he4.output.density");
@@ -224,6 +249,88 @@ void readenc_mode2(Run &r) {
   r.grid.hy = 2.0 * r.p.ymax / r.p.ny;
   r.grid.hz = 2.0 * r.p.zmax / r.p.nz;
   r.grid.xmax = r.p.xmax, r.grid.ymax = r.p.ymax, r.grid.zmax = r.p.zmax;
+}
+
+// trilinear value of a grid field at a point, zero outside cells 1..n-1
+// (interpola3denx with blend_103, sorteo.f90:49-83)
+double trilinear(const std::vector<double> &f, const Run &r, const double xyz[3]) {
+  const double lo[3] = {-r.p.xmax, -r.p.ymax, -r.p.zmax}, hh[3] = {r.grid.hx, r.grid.hy, r.grid.hz};
+  const int n[3] = {r.p.nx, r.p.ny, r.p.nz};
+  int ic[3];
+  double w[3];
+  for (int c = 0; c < 3; c++) {
+    const double a = (xyz[c] - lo[c]) / hh[c] + 1.0;
+    ic[c] = (int)a;
+    w[c] = a - ic[c];
+    if (ic[c] >= n[c] || ic[c] <= 0) return 0.0;
+  }
+  auto at = [&](int dx, int dy, int dz) {
+    return f[((size_t)(ic[2] - 1 + dz) * r.p.ny + (ic[1] - 1 + dy)) * r.p.nx + (ic[0] - 1 + dx)];
+  };
+  double v = 0.0;
+  for (int dz = 0; dz < 2; dz++)
+    for (int dy = 0; dy < 2; dy++)
+      for (int dx = 0; dx < 2; dx++)
+        v += (dx ? w[0] : 1.0 - w[0]) * (dy ? w[1] : 1.0 - w[1]) * (dz ? w[2] : 1.0 - w[2]) * at(dx, dy, dz);
+  return v;
+}
+
+// readenc mode 0 (readenc.f90:78-92) and the start it implies
+// (DFT4He3d.f90:585-617): psi = sqrt(den) exp(i (lx x + ly y + lz z)); the
+// test particles drawn by rejection from denx inside [xi,xf]x[yi,yf]x[zi,zf]
+// (sorteo.f90:1-28, here from a seeded generator), all moving at v0
+void readenc_mode0(Run &r) {
+  std::vector<double> den, denx;
+  he4io::GridHeader gx;
+  he4io::read_density(r.filedenin, &r.grid, &den);
+  he4io::read_density(r.fileimpin, &gx, &denx);
+  if (r.grid.nx != r.p.nx || r.grid.ny != r.p.ny || r.grid.nz != r.p.nz || gx.nx != r.p.nx || gx.ny != r.p.ny ||
+      gx.nz != r.p.nz)
+    die("the density files' grid does not match the namelist");
+  r.grid.hx = 2.0 * r.p.xmax / r.p.nx;
+  r.grid.hy = 2.0 * r.p.ymax / r.p.ny;
+  r.grid.hz = 2.0 * r.p.zmax / r.p.nz;
+  r.grid.xmax = r.p.xmax, r.grid.ymax = r.p.ymax, r.grid.zmax = r.p.zmax;
+  r.psi.resize(den.size());
+  for (int iz = 0; iz < r.p.nz; iz++)
+    for (int iy = 0; iy < r.p.ny; iy++)
+      for (int ix = 0; ix < r.p.nx; ix++) {
+        const double x = -r.p.xmax + r.grid.hx * ix, y = -r.p.ymax + r.grid.hy * iy, z = -r.p.zmax + r.grid.hz * iz;
+        const double aux = x * r.xlamdax + y * r.xlamday + z * r.xlamdaz;
+        const size_t t = ((size_t)iz * r.p.ny + iy) * r.p.nx + ix;
+        r.psi[t] = std::sqrt(den[t]) * std::complex<double>(std::cos(aux), std::sin(aux));
+      }
+  double dmax = 0.0;
+  for (double v : denx) dmax = std::max(dmax, v);
+  if (!(dmax > 0.0)) die("sorteo: the impurity density is zero everywhere");
+  const int np = r.p.n_par;
+  r.npar = np;
+  r.rimp.assign(3 * (size_t)np, 0.0);
+  r.vimp.assign(3 * (size_t)np, 0.0);
+  std::mt19937_64 gen(r.seed);
+  std::uniform_real_distribution<double> u(0.0, 1.0);
+  const double lo[3] = {r.xi, r.yi, r.zi}, hi[3] = {r.xf, r.yf, r.zf};
+  for (int i = 0; i < np; i++) {
+    double xyz[3];
+    for (long tries = 0;; tries++) {
+      if (tries > 100000000L) die("sorteo: no particle accepted in 1e8 draws (box outside denx?)");
+      for (int c = 0; c < 3; c++) xyz[c] = u(gen) * (hi[c] - lo[c]) + lo[c];
+      const double dum = u(gen) * dmax;
+      if (dum < trilinear(denx, r, xyz)) break;
+    }
+    for (int c = 0; c < 3; c++) {
+      r.rimp[(size_t)c * np + i] = xyz[c];
+      r.vimp[(size_t)c * np + i] = r.v0[c] * kKtops;  // A/ps -> A*K
+    }
+  }
+  // density.000.dat / densityx.000.dat of the start (DFT4He3d.f90:611-617)
+  he4io::PrintInfo info;
+  info.time = 0.0;
+  info.iprint = r.binary ? -3 : 3;
+  info.iter = 0;
+  info.paflv = r.deltatps;
+  he4io::write_psi("density.000.dat", info, r.grid, r.psi);
+  he4io::write_impurity("densityx.000.dat", info, r.grid, r.psi, r.npar, r.rimp, r.vimp);
 }
 
 void printoutc(he4_handle *h, Run &r, double time, int iprint, const std::string &f, const std::string &f1,
@@ -367,7 +474,10 @@ int main(int argc, char **argv) {
     std::stringstream ss;
     ss << std::cin.rdbuf();
     load_input(r, ss.str());
-    readenc_mode2(r);
+    if (r.mode == 0)
+      readenc_mode0(r);
+    else
+      readenc_mode2(r);
   } catch (const std::exception &e) {
     die(e.what());
   }

@@ -156,3 +156,59 @@ def test_namelist_and_readenc(he4run, tmp_path):
     vr.write_text(" 3.0 1.0\n 3.1 0.5\n 3.3 0.2\n 3.4 0.1\n")
     r = subprocess.run([he4run, "--print-input"], input=good, capture_output=True, text=True)
     assert r.returncode != 0 and "uniformly" in r.stderr
+
+
+def write_density(path, xmax, h, n, den):
+    """A readenc mode-0 density file: '#' comment lines (titols), the header
+    xmax,ymax,zmax,hx,hy,hz,nx,ny,nz,limp,ximp,yimp,zimp, then den(nx,ny,nz)."""
+    with open(path, "w") as f:
+        f.write("# synthetic density\n")
+        f.write(f" {xmax!r} {xmax!r} {xmax!r} {h!r} {h!r} {h!r} {n} {n} {n} T 0.0 0.0 0.0\n")
+        f.write("\n".join(f" {v:.17E}" for v in den.reshape(-1)))
+        f.write("\n")
+
+
+def test_readenc_mode0_start(he4run, tmp_path):
+    """mode=0 (the shipped inputs): psi = sqrt(den) times the constraint phase,
+    test particles drawn from denx inside [xi,xf]x[yi,yf]x[zi,zf], all at v0
+    (DFT4He3d.f90:585-617, readenc.f90:78-92, sorteo.f90:1-28); the draw is
+    seeded here, the reference's is not."""
+    n, h = 16, 0.5
+    xmax = n * h / 2
+    x = -xmax + h * np.arange(n)
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    den = 0.0218 / (1 + np.exp((np.sqrt(X ** 2 + Y ** 2 + Z ** 2) - 3.0) / 0.5))
+    denx = np.where((np.abs(X - 1.0) < 0.6) & (np.abs(Y) < 0.6) & (np.abs(Z + 0.5) < 0.6), 1.0, 0.0)
+    d = str(tmp_path)
+    write_density(os.path.join(d, "den.inp"), xmax, h, n, den)
+    write_density(os.path.join(d, "denx.inp"), xmax, h, n, denx)
+    nml = f""" &input nx={n}, ny={n}, nz={n}, xmax={xmax!r}, ymax={xmax!r}, zmax={xmax!r},
+   mode=0, filedenin='den.inp', fileimpin='denx.inp', N_par=200, npd=7, icon=13,
+   xi=-2.d0, xf=3.d0, yi=-2.d0, yf=2.d0, zi=-2.d0, zf=2.d0, v0z=1.5d0, xlamda=0.3d0,
+   deltatps=1.d-3, niter=0, seed=7 /
+"""
+    r = subprocess.run([he4run, "--print-input"], input=nml, capture_output=True, text=True, cwd=d)
+    assert r.returncode == 0, r.stderr
+    kv = dict(t.split("=") for t in r.stdout.split())
+    assert kv["icon"] == "13" and kv["n_par"] == "200"
+    # |psi|^2 = den whatever the phase
+    assert float(kv["psi_norm2"]) == pytest.approx(float(np.sum(den)), rel=1e-13)
+    # every particle at v0 (A/ps -> A*K), drawn where denx > 0 and inside the box
+    assert float(kv["vimp_last"]) == pytest.approx(1.5 * 7.63822291, rel=1e-15)
+    r0 = float(kv["rimp0"])
+    assert 0.4 - h <= r0 <= 1.6 + h
+    # the start's density.000.dat holds that psi
+    assert os.path.exists(os.path.join(d, "density.000.dat"))
+    # the draw is reproducible for a seed and changes with it
+    again = subprocess.run([he4run, "--print-input"], input=nml, capture_output=True, text=True, cwd=d)
+    assert dict(t.split("=") for t in again.stdout.split())["rimp0"] == kv["rimp0"]
+    other = subprocess.run([he4run, "--print-input"], input=nml.replace("seed=7", "seed=8"), capture_output=True,
+                           text=True, cwd=d)
+    assert dict(t.split("=") for t in other.stdout.split())["rimp0"] != kv["rimp0"]
+    # mode 0 needs the particle box; mode 1 does not exist in the reference either
+    bad = nml.replace("xi=-2.d0, ", "")
+    r = subprocess.run([he4run, "--print-input"], input=bad, capture_output=True, text=True, cwd=d)
+    assert r.returncode != 0 and "xi" in r.stderr
+    r = subprocess.run([he4run, "--print-input"], input=nml.replace("mode=0", "mode=1"), capture_output=True,
+                       text=True, cwd=d)
+    assert r.returncode != 0 and "not programmed" in r.stderr
