@@ -120,3 +120,75 @@ def test_driver_spherical_bubble(pkg, tmp_path):
         tt, rr = map(float, l.split())
         assert tt == pytest.approx(t, abs=1e-9)
         assert rr == pytest.approx(rb, rel=1e-9)
+
+
+def read_particles(path):
+    body = [l for l in open(path).read().splitlines() if not l.startswith("#")]
+    n = int(body[0])
+    vals = np.array([float(l) for l in body[1:1 + 6 * n]])
+    return n, vals[:3 * n].reshape(3, n), vals[3 * n:].reshape(3, n)
+
+
+def test_driver_shipped_style_start(pkg, tmp_path):
+    """The options of the shipped inputs (data_files/input_He2S.*) on a small
+    grid: mode=0 start from density files, icon=13, npd=13, ironx=3, an
+    absorbing layer, a non-power-of-two axis (generic FFT path), and a pair
+    potential given as sampled V(r) (vrfile).  The driver's run equals the
+    library's run from the start it wrote (density.000.dat / densityx.000.dat)."""
+    import ctypes as C
+    w = pkg.workloads
+    d = str(tmp_path)
+    nx, nz, h = 48, 40, 0.6
+    p = w.make_params(nx, h, 400, npd=13, nz=nz)
+    p.icon = 13
+    p.ironx = 3
+    p.lambdah, p.tzmean, p.tzsurf = 2.0, 10.0, 1.0
+    x, y, z = w.grid_axes(p)
+    den = np.abs(w.droplet_psi(p, 300)) ** 2
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    denx = np.exp(-((X - 0.3) ** 2 + Y ** 2 + (Z - 1.0) ** 2) / 0.5)
+    for name, f in (("den.inp", den), ("denx.inp", denx)):
+        with open(os.path.join(d, name), "w") as fh:
+            fh.write(f"# start\n {p.xmax!r} {p.ymax!r} {p.zmax!r} {h!r} {h!r} {h!r} {p.nx} {p.ny} {p.nz} T 0. 0. 0.\n")
+            fh.write("\n".join(f" {v:.17E}" for v in f.reshape(-1)) + "\n")
+    dr = 0.01
+    r = p.r_cutoff + dr * np.arange(int((60.0 - p.r_cutoff) / dr) + 1)
+    v = p.morse_d * ((1.0 - np.exp(-p.morse_alpha * (r - p.morse_re))) ** 2 - 1.0)
+    with open(os.path.join(d, "vr.dat"), "w") as fh:
+        fh.write("".join(f" {a:.17E} {b:.17E}\n" for a, b in zip(r, v)))
+    nml = f""" &input nx={p.nx}, ny={p.ny}, nz={p.nz}, xmax={p.xmax!r}, ymax={p.ymax!r}, zmax={p.zmax!r},
+   n4=300, mode=0, filedenin='den.inp', fileimpin='denx.inp', core4='OTC', npd=13, icon=13,
+   N_par={p.n_par}, mimpur={p.mimpur!r}, ironx=3, Lambdah=2.d0, tzmean=10.d0, tzsurf=1.d0,
+   xi=-1.5d0, xf=2.d0, yi=-1.5d0, yf=1.5d0, zi=-0.5d0, zf=2.5d0, v0z=-1.d0, seed=3,
+   deltatps=1.d-3, niter=6, pener=3, pcurr=0, selec_gs='He2S_fci', vrfile='vr.dat',
+   r_cutoff_gs={p.r_cutoff!r}, umax_gs={p.umax!r}, nq={p.nq} /
+"""
+    res = subprocess.run([os.path.join(PKG, "he4run")], input=nml, capture_output=True, text=True, cwd=d)
+    assert res.returncode == 0, res.stderr[-2000:]
+    assert "TOTAL energy (He+X)" in res.stdout
+    psi0 = read_psi(os.path.join(d, "density.000.dat"), den.shape)
+    assert np.allclose(np.abs(psi0) ** 2, den, rtol=1e-14, atol=1e-30)
+    n, r0, v0 = read_particles(os.path.join(d, "densityx.000.dat"))
+    assert n == p.n_par and np.all(v0[2] == -7.63822291) and np.all(v0[:2] == 0)
+    got = read_psi(os.path.join(d, "he4.output.density"), den.shape)
+    q = pkg.abi.He4Params.from_buffer_copy(p)
+    q.pot_kind = pkg.abi.HE4_POT_RTABLE
+    vv = np.ascontiguousarray(v)
+    q.vr_table = vv.ctypes.data_as(C.POINTER(C.c_double))
+    q.n_vr, q.vr_r0, q.vr_dr = vv.size, float(r[0]), (r[-1] - r[0]) / (r.size - 1)
+    dt = w.deltat_fs(1.0)
+    with pkg.He4Step(q) as g:
+        g.set_state(psi0, r0, v0)
+        g.field()
+        g.energy()
+        for it in range(1, 7):
+            if it <= 3:
+                g.steprk(dt)
+            else:
+                g.steppc(dt)
+            if it % 3 == 0:
+                g.energy()
+        want = g.get_state()[0]
+    # the files hold 17 significant digits, so the start differs from the
+    # driver's in the last place
+    assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
