@@ -83,6 +83,31 @@ def test_fp32_field_and_energy_terms(pkg, ora, c1):
     o.close()
 
 
+def test_fp32_icon13_against_oracle(pkg, ora):
+    """The FP32 form with zero-padded stencils (icon=13: FP64 intermediate
+    grids, the force from transformed gradients) against the FP64 oracle:
+    the tolerances of the periodic case."""
+    w = pkg.workloads
+    p = w.make_params(64, 0.6, 256)
+    p.icon = 13
+    psi = w.droplet_psi(p, 600)
+    r, v = w.particles(256, 1234, 100.0)
+    o = ora.Oracle(p)
+    o.set_state(psi, r, v)
+    o.field()
+    with pkg.He4Step(fp32_params(pkg, p)) as g:
+        g.set_state(psi, r, v)
+        g.field()
+        for name in ("den", "denx", "dxden", "dzden", "penalty"):
+            assert rel(g.get_field(name), o.get_field(name)) < 1e-11, name
+        for name in pkg.abi.FIELDS:
+            assert rel(g.get_field(name), o.get_field(name)) < 5e-6, name
+        assert rel(g.get_state()[3], o.get_state()[3]) < 5e-6
+        eg, eo = g.energy(), o.energy()
+        assert abs(eg["etot"] - eo["etot"]) <= 1e-7 * abs(eo["etot"])
+    o.close()
+
+
 def test_fp32_steps_against_fp64(pkg, c1):
     p, psi, r, v, _ = c1
     dt = pkg.workloads.deltat_fs(1.0)
