@@ -18,6 +18,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include <cuda_pipeline.h>
@@ -637,8 +638,9 @@ static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse
     a.map = map;
     const long ntiles = (total + W - 1) / W;
     // one wave of persistent CTAs: as many as fit on the SMs at once
-    static int per_sm[2] = {0, 0};
-    int &ps = per_sm[inverse ? 1 : 0];
+    // per instantiation; handles on other host threads may read it at once
+    static std::atomic<int> per_sm[2];
+    int ps = per_sm[inverse ? 1 : 0].load(std::memory_order_relaxed);
     if (ps == 0) {
       int dev = 0, nsm = 0, occ = 0;
       cudaGetDevice(&dev);
@@ -650,6 +652,7 @@ static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_yz_pipe<NN, N1_, false, C2>, kRegThreads,
                                                       smem_yz_reg<NN, N1_, C2>());
       ps = std::max(1, occ) * std::max(1, nsm);
+      per_sm[inverse ? 1 : 0].store(ps, std::memory_order_relaxed);
     }
     dim3 grid((unsigned)std::min<long>(ntiles, std::max(1, ps / nb)), nb);
     if (inverse)
@@ -809,8 +812,8 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
       constexpr int W = kRegThreads / N1_;
       a.map.W = W;
       const long ntiles = (total + W - 1) / W;
-      static int per_sm[2] = {0, 0};
-      int &ps = per_sm[single ? 1 : 0];
+      static std::atomic<int> per_sm[2];
+      int ps = per_sm[single ? 1 : 0].load(std::memory_order_relaxed);
       if (ps == 0) {
         int dev = 0, nsm = 0, occ = 0;
         cudaGetDevice(&dev);
@@ -822,6 +825,7 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zconv_pipe<NN, N1_, false, C2>, kRegThreads,
                                                         smem_zpipe<NN, N1_, C2>());
         ps = std::max(1, occ) * std::max(1, nsm);
+        per_sm[single ? 1 : 0].store(ps, std::memory_order_relaxed);
       }
       dim3 grid(nb, (unsigned)std::min<long>(ntiles, std::max(1, ps / nb)));
       if (single) {
