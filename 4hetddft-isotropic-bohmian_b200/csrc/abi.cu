@@ -1,4 +1,5 @@
 // abi.cu -- the extern "C" entry points of include/he4_tddft.h.
+#include <limits.h>
 #include <math.h>
 #include <stdarg.h>
 #include <stdlib.h>
@@ -103,7 +104,7 @@ static void free_all(Handle *h) {
                   h->dyden, h->dzden, h->penalty, h->corr, h->denx, h->psix, h->hpsix, h->uimp, h->fx, h->fy,
                   h->fz, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], h->counts, h->rimp, h->vimp, h->aimp,
                   h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
-                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->bub, h->box,
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->bub, h->box, h->gred,
                   h->k32[0], h->k32[1], h->k32[2], h->k32[3], h->dsym32};
   for (void *p : ptrs) cudaFree(p);
   for (int i = 0; i < 9; i++) cudaFree(h->g32[i]);
@@ -128,7 +129,7 @@ static int create(const he4_params *pin, Handle *h) {
     set_error("no CUDA device");
     return HE4_E_NODEVICE;
   }
-  if (pin->device < 0 || pin->device >= ndev) {
+  if (pin->device < 0 || pin->device >= ndev || pin->device >= kMaxDevices) {
     set_error("device %d out of range (%d devices)", pin->device, ndev);
     return HE4_E_ARG;
   }
@@ -180,6 +181,16 @@ static int create(const he4_params *pin, Handle *h) {
   for (double **f : rfields) HE4_TRY(dalloc(f, N));
   HE4_TRY(dalloc(&h->counts, N));
   HE4_TRY(dalloc(&h->box, 1));
+  HE4_TRY(dalloc(&h->gred, 1));
+  {
+    GridRed g0;
+    memset(&g0, 0, sizeof(g0));
+    for (int d = 0; d < 3; d++) {
+      g0.box[d] = INT_MAX;
+      g0.box[3 + d] = INT_MIN;
+    }
+    HE4_CUDA_TRY(cudaMemcpy(h->gred, &g0, sizeof(GridRed), cudaMemcpyHostToDevice));
+  }
   for (int i = 0; i < 6; i++) HE4_TRY(dalloc(&h->spec[i], H));
   double **pfields[] = {&h->rimp, &h->vimp, &h->aimp, &h->rimpold[0], &h->rimpold[1], &h->rimpold[2],
                         &h->vimpold[0], &h->vimpold[1], &h->vimpold[2], &h->aimpold[0], &h->aimpold[1],
@@ -354,11 +365,30 @@ int he4_snapshot_begin(he4_handle *hh) {
     h->snap_pending = 0;
   }
   if (!h->snap_dev) {
-    HE4_CUDA_TRY(cudaMalloc((void **)&h->snap_dev, sizeof(double) * n));
-    HE4_CUDA_TRY(cudaMallocHost((void **)&h->snap_host, sizeof(double) * n));
-    HE4_CUDA_TRY(cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
-    HE4_CUDA_TRY(cudaEventCreateWithFlags(&h->snap_taken, cudaEventDisableTiming));
-    HE4_CUDA_TRY(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+    // all five resources or none: a partial set is released and the
+    // handle keeps none, so the next call starts over
+    double *dev = nullptr, *host = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t taken = nullptr, done = nullptr;
+    cudaError_t ce = cudaMalloc((void **)&dev, sizeof(double) * n);
+    if (ce == cudaSuccess) ce = cudaMallocHost((void **)&host, sizeof(double) * n);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&taken, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+    if (ce != cudaSuccess) {
+      if (done) cudaEventDestroy(done);
+      if (taken) cudaEventDestroy(taken);
+      if (st) cudaStreamDestroy(st);
+      if (host) cudaFreeHost(host);
+      if (dev) cudaFree(dev);
+      set_error("he4_snapshot_begin allocation: %s", cudaGetErrorString(ce));
+      return HE4_E_CUDA;
+    }
+    h->snap_dev = dev;
+    h->snap_host = host;
+    h->snap_stream = st;
+    h->snap_taken = taken;
+    h->snap_done = done;
   }
   double *d = h->snap_dev;
   HE4_CUDA_TRY(cudaMemcpyAsync(d, h->psi, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
@@ -682,6 +712,8 @@ int he4_fft_c2r(he4_handle *hh, const double *in, double *out) {
   return HE4_OK;
 }
 
+constexpr int kBenchKernels = 11;
+
 static int launch_bench(Handle *h, int which) {
   switch (which) {
     case 0: {
@@ -707,6 +739,8 @@ static int launch_bench(Handle *h, int which) {
     }
     case 7: return launch_grad(h);
     case 8: return launch_pot4_merged(h);
+    case 9: return launch_pot4_merged_f32(h);
+    case 10: return fft_x_c2r_f32_only(h, h->spec[1], h->g32[8]);
     default: set_error("unknown kernel id %d", which); return HE4_E_ARG;
   }
 }
@@ -718,20 +752,33 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
     set_error("invalid arguments");
     return HE4_E_ARG;
   }
-  static const char *names[9] = {"k_fft_z_conv",  "k_fft_y",           "k_fft_x_r2c", "k_fft_x_c2r",
-                                 "k_fft_z_plain", "k_fft_z_conv_nokern", "k_fft_z_conv_3out", "k_grad",
-                                 "k_pot4_merged"};
+  // kernel families the ids launch (the template arguments follow the grid
+  // and the form; ncu's launch lists name them in full)
+  static const char *names[kBenchKernels] = {
+      "k_zconv (z conv, 1 output)", "k_yz_pipe (y pass)",           "k_xr2c_reg (x R2C)",
+      "k_xc2r_reg (x C2R)",         "k_zconv (z pass, no multiply)", "k_zconv (z conv, no kernel)",
+      "k_zconv (z conv, 3 outputs)", "k_grad_z (density gradient)",  "k_pot4_merged_z (pot4, FP64 grids)",
+      "k_pot4_merged_z (pot4, float grids)", "k_xc2r_reg (x C2R, float rows)"};
   const double H = (double)h->H, N = (double)h->N;
   // algorithmic bytes: read input once, write output once (+ the real
   // kernel); c and k are the sizes of a spectrum and a kernel element
   const double c = h->fp32 ? 8 : 16, k = h->fp32 ? 4 : 8;
-  const double bytes[9] = {c * H + k * H + c * H, 2 * c * H, 8 * N + c * H, c * H + 8 * N,
-                           2 * c * H,             2 * c * H, c * H + 3 * (k * H + c * H),
-                           // stencils: den in, three gradients out; lin, den, dencg, h0..h2 in, pot4 out
-                           4 * 8 * N,             7 * 8 * N};
-  if (which < 0 || which > 8) {
+  const double bytes[kBenchKernels] = {
+      c * H + k * H + c * H, 2 * c * H, 8 * N + c * H, c * H + 8 * N, 2 * c * H, 2 * c * H,
+      c * H + 3 * (k * H + c * H),
+      // stencils: den in, three gradients out; lin, den, dencg, h0..h2 in, pot4 out
+      4 * 8 * N, 7 * 8 * N,
+      // float grids: lin, dencg, h0..h2 (4 B), den in and pot4 out (8 B)
+      5 * 4 * N + 2 * 8 * N,
+      // half spectrum in, float rows out
+      c * H + 4 * N};
+  if (which < 0 || which >= kBenchKernels) {
     set_error("unknown kernel id %d", which);
     return HE4_E_ARG;
+  }
+  if ((which == 9 || which == 10) && !h->real32) {
+    set_error("kernel id %d needs the FP32-convolution form with float grids", which);
+    return HE4_E_STATE;
   }
   HE4_TRY(launch_bench(h, which));  // warm-up
   cudaEvent_t e0, e1;

@@ -61,6 +61,10 @@ __host__ __device__ __forceinline__ double2 cmuli(double2 a) {
   return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
 }
 
+// Per-device host caches (launch attributes, occupancy, scratch addresses)
+// are arrays over the device ordinal; he4_create refuses ordinals past it.
+constexpr int kMaxDevices = 64;
+
 // ---------------------------------------------------------------------------
 // FFT plan
 // ---------------------------------------------------------------------------
@@ -107,6 +111,18 @@ struct Box {
 };
 struct BoxPair {
   Box cur, prev;
+};
+
+// Particle kernels run on up to kPartMaxCta CTAs of kPartThreads threads
+// (a fixed cap, not the SM count, so their reductions give the same bits
+// on every device).  Their grid-wide reductions keep per-CTA partials and
+// a last-CTA counter here; box holds the running NGP min/max of k_box_find.
+constexpr int kPartThreads = 256;
+constexpr int kPartMaxCta = 296;
+struct GridRed {
+  double part[9 * kPartMaxCta];
+  unsigned count[4];  // 0: box, 1: corrector errors, 2: means
+  int box[6];         // min x, y, z, max x, y, z; reset by the last CTA
 };
 
 // ---------------------------------------------------------------------------
@@ -188,6 +204,7 @@ struct Handle {
   int ioldp[3] = {0, 1, 2}, ioldh[2] = {0, 1}, ioldr[3] = {0, 1, 2}, ioldv[3] = {0, 1, 2}, iolda[2] = {0, 1};
 
   // reductions
+  GridRed *gred = nullptr;    // particle-kernel partials, counters, box scratch
   double *red = nullptr;      // partial sums workspace
   double *scal = nullptr;     // device scalars (errors, energies, means)
   double *hscal = nullptr;    // pinned host mirror of scal
@@ -281,6 +298,7 @@ __device__ __forceinline__ void force_range(const BoxPair *bp, int axis, int n, 
 int fft_z_only(Handle *h, double2 *buf, bool inverse);
 // x pass alone (R2C: rin -> cout; C2R: cin -> rout)
 int fft_x_only(Handle *h, const double *rin, double2 *cout, const double2 *cin, double *rout, bool inverse);
+int fft_x_c2r_f32_only(Handle *h, const double2 *cin, float *rout);
 
 int setup_kernels(Handle *h);
 // element-wise FP64 <-> FP32 conversion of n reals on the handle's stream
@@ -302,6 +320,7 @@ int launch_grad(Handle *h);
 // the merged evaluation may keep float intermediate grids (Handle::real32)
 bool real32_ok(const Handle *h);
 int launch_pot4_merged(Handle *h);
+int launch_pot4_merged_f32(Handle *h);
 // potenimp + poten + forceimp; marks the fields valid.  split = false takes
 // the merged form when the z length allows it.
 int field_all(Handle *h, bool split = false);

@@ -100,7 +100,10 @@ static int launch_diag(const double *den, const DiagArgs &a, double dxyz, double
 // Device address of g_diag_noalloc_part, looked up once per device (with that
 // device current) the first time he4_diagnostics_noalloc runs on it.  In host
 // code the symbol is only a stand-in; kernels must be given this address.
-constexpr int kMaxDevices = 64;
+// The cached address belongs to the device's primary context as it was at
+// that first call: after cudaDeviceReset (which tears the context down, and
+// the module with it) the address is stale, so a host that resets a device
+// must not call he4_diagnostics_noalloc on it again in the same process.
 static std::mutex g_noalloc_mu;
 static double *g_noalloc_ptr[kMaxDevices] = {nullptr};
 

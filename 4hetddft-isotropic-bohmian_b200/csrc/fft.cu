@@ -382,25 +382,35 @@ static size_t smem_yz(int n, int W) {
   return sizeof(double2) * (2 * (size_t)n * W + n) + sizeof(long) * W + 2 * sizeof(int) * W;
 }
 
-// The dynamic shared memory limits of the generic-path kernels are
-// process-wide; they only ever grow, to the widest tiles any plan uses.
+// The dynamic shared memory limits of the generic-path kernels are set per
+// device (a cudaFuncSetAttribute call applies to the current device only);
+// per device they only ever grow, to the widest tiles any plan there uses.
+// A maximum is recorded only after the attribute call succeeded, so a failed
+// call is retried by the next plan.
 static int generic_attrs(const FftPlan &P) {
   static std::mutex mu;
-  static size_t max_x = 0, max_y = 0, max_z = 0;
+  static size_t max_x[kMaxDevices] = {0}, max_y[kMaxDevices] = {0}, max_z[kMaxDevices] = {0};
+  int dev = 0;
+  HE4_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device ordinal %d beyond the %d this library supports", dev, kMaxDevices);
+    return HE4_E_ARG;
+  }
   std::lock_guard<std::mutex> lock(mu);
-  if (smem_x(P) > max_x) {
-    max_x = smem_x(P);
-    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_x));
-    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_x));
+  const size_t sx = smem_x(P), sy = smem_yz(P.ny, P.wy), sz = smem_yz(P.nz, P.wz);
+  if (sx > max_x[dev]) {
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
+    max_x[dev] = sx;
   }
-  if (smem_yz(P.ny, P.wy) > max_y) {
-    max_y = smem_yz(P.ny, P.wy);
-    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_y));
-    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_y));
+  if (sy > max_y[dev]) {
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
+    max_y[dev] = sy;
   }
-  if (smem_yz(P.nz, P.wz) > max_z) {
-    max_z = smem_yz(P.nz, P.wz);
-    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_z));
+  if (sz > max_z[dev]) {
+    HE4_CUDA_TRY(cudaFuncSetAttribute(k_fft_z_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
+    max_z[dev] = sz;
   }
   return HE4_OK;
 }
@@ -637,13 +647,13 @@ static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse
     map.W = W;
     a.map = map;
     const long ntiles = (total + W - 1) / W;
-    // one wave of persistent CTAs: as many as fit on the SMs at once
-    // per instantiation; handles on other host threads may read it at once
-    static std::atomic<int> per_sm[2];
-    int ps = per_sm[inverse ? 1 : 0].load(std::memory_order_relaxed);
+    // one wave of persistent CTAs: as many as fit on the SMs at once, per
+    // instantiation and device; handles on other host threads may read it
+    static std::atomic<int> per_sm[kMaxDevices][2];
+    const int dev = h->dev;
+    int ps = per_sm[dev][inverse ? 1 : 0].load(std::memory_order_relaxed);
     if (ps == 0) {
-      int dev = 0, nsm = 0, occ = 0;
-      cudaGetDevice(&dev);
+      int nsm = 0, occ = 0;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
       if (inverse)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_yz_pipe<NN, N1_, true, C2>, kRegThreads,
@@ -652,7 +662,7 @@ static int yz_reg(Handle *h, int nb, double2 *const *buf, int axis, bool inverse
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_yz_pipe<NN, N1_, false, C2>, kRegThreads,
                                                       smem_yz_reg<NN, N1_, C2>());
       ps = std::max(1, occ) * std::max(1, nsm);
-      per_sm[inverse ? 1 : 0].store(ps, std::memory_order_relaxed);
+      per_sm[dev][inverse ? 1 : 0].store(ps, std::memory_order_relaxed);
     }
     dim3 grid((unsigned)std::min<long>(ntiles, std::max(1, ps / nb)), nb);
     if (inverse)
@@ -812,11 +822,11 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
       constexpr int W = kRegThreads / N1_;
       a.map.W = W;
       const long ntiles = (total + W - 1) / W;
-      static std::atomic<int> per_sm[2];
-      int ps = per_sm[single ? 1 : 0].load(std::memory_order_relaxed);
+      static std::atomic<int> per_sm[kMaxDevices][2];  // per instantiation and device
+      const int dev = h->dev;
+      int ps = per_sm[dev][single ? 1 : 0].load(std::memory_order_relaxed);
       if (ps == 0) {
-        int dev = 0, nsm = 0, occ = 0;
-        cudaGetDevice(&dev);
+        int nsm = 0, occ = 0;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         if (single)
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zconv_pipe<NN, N1_, true, C2>, kRegThreads,
@@ -825,7 +835,7 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zconv_pipe<NN, N1_, false, C2>, kRegThreads,
                                                         smem_zpipe<NN, N1_, C2>());
         ps = std::max(1, occ) * std::max(1, nsm);
-        per_sm[single ? 1 : 0].store(ps, std::memory_order_relaxed);
+        per_sm[dev][single ? 1 : 0].store(ps, std::memory_order_relaxed);
       }
       dim3 grid(nb, (unsigned)std::min<long>(ntiles, std::max(1, ps / nb)));
       if (single) {
@@ -931,6 +941,13 @@ int fft_z_sum(Handle *h, int nterm, const ZTerm *terms, double2 *out) {
 int fft_z_only(Handle *h, double2 *buf, bool inverse) {
   ZOp op{buf, buf, nullptr, 1.0, -1, inverse ? 2 : 1};
   return fft_z_conv(h, 1, &op);
+}
+
+// the inverse x pass alone with float output rows (FP32-convolution form)
+int fft_x_c2r_f32_only(Handle *h, const double2 *cin, float *rout) {
+  double2 *ci[1] = {const_cast<double2 *>(cin)};
+  void *ro[1] = {rout};
+  return x_pass_v(h, 1, nullptr, nullptr, ci, ro, true, nullptr, XLoad(), true);
 }
 
 int fft_x_only(Handle *h, const double *rin, double2 *cout, const double2 *cin, double *rout, bool inverse) {

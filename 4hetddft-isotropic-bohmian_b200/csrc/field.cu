@@ -662,7 +662,21 @@ static int field_poten_merged_f32(Handle *h) {
     float *out[1] = {sl};  // lin (s is consumed)
     HE4_TRY(fft_c2r_f32(h, 1, sp, out));
   }
-  const float *h0 = otc ? hv[0] : nullptr, *h1 = otc ? hv[1] : nullptr, *h2 = otc ? hv[2] : nullptr;
+  return launch_pot4_merged_f32(h);
+}
+
+// pot4 of the FP32-convolution form's merged evaluation: lin (in g32[8]),
+// dencg (g32[0]) and h_i (g32[5..7]) are float grids, den and pot4 double
+int launch_pot4_merged_f32(Handle *h) {
+  if (!h->real32) {
+    set_error("the float-grid pot4 stencil needs the FP32-convolution form's float grids");
+    return HE4_E_STATE;
+  }
+  const Geo g = geo(h);
+  const OtArgs ot = ot_args(h);
+  const bool otc = (h->p.core4 == HE4_CORE_OTC);
+  const float *sl = h->g32[8], *dencg = h->g32[0];
+  const float *h0 = otc ? h->g32[5] : nullptr, *h1 = otc ? h->g32[6] : nullptr, *h2 = otc ? h->g32[7] : nullptr;
   if (h->st.m == 3) {
     if (otc)
       k_pot4_merged_z<true, 3, kZBp, float, false><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(sl, h->den, dencg, h0, h1,

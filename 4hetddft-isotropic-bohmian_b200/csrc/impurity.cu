@@ -51,12 +51,17 @@ __global__ void k_deposit(const double *__restrict__ rimp, unsigned int *counts,
     atomicAdd(counts + ((size_t)c[2] * a.ny + c[1]) * a.nx + c[0], 1u);
 }
 
-// One CTA: prev = cur; cur = NGP cells of all particles widened by `iron`,
-// or the whole grid when the widened box plus 2m reaches a face.
-__global__ void k_box_find(const double *__restrict__ rimp, DepArgs a, int iron, int m, BoxPair *bp) {
-  __shared__ int sh[6][32];
+// prev = cur; cur = NGP cells of all particles widened by `iron`, or the
+// whole grid when the widened box plus 2m reaches a face.  Every CTA folds
+// the cells of its particles into the GridRed min/max scratch with integer
+// atomics (exact, so the order does not matter); the CTA that finishes
+// last forms the box and resets the scratch for the next launch.
+__global__ void __launch_bounds__(kPartThreads) k_box_find(const double *__restrict__ rimp, DepArgs a, int iron, int m,
+                                                           GridRed *gr, BoxPair *bp) {
+  __shared__ int sh[6][kPartThreads / 32];
+  __shared__ int last;
   int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-  for (int p = threadIdx.x; p < a.npar; p += blockDim.x) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.npar; p += gridDim.x * blockDim.x) {
     int c[3];
     if (ngp_cell3(a, rimp[p], rimp[a.npar + p], rimp[2 * a.npar + p], c)) {
 #pragma unroll
@@ -81,23 +86,41 @@ __global__ void k_box_find(const double *__restrict__ rimp, DepArgs a, int iron,
     }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int d = 0; d < 3; d++)
+    for (int d = 0; d < 3; d++) {
       for (int w = 1; w < nw; w++) {
         sh[d][0] = min(sh[d][0], sh[d][w]);
         sh[3 + d][0] = max(sh[3 + d][0], sh[3 + d][w]);
       }
-    Box b;
-    b.full = 0;
-    b.empty = (sh[0][0] == INT_MAX);
-    const int n[3] = {a.nx, a.ny, a.nz};
-    for (int d = 0; d < 3; d++) {
-      b.lo[d] = b.empty ? 0 : sh[d][0] - iron;
-      b.hi[d] = b.empty ? -1 : sh[3 + d][0] + iron;
-      if (!b.empty && (b.lo[d] - 2 * m < 0 || b.hi[d] + 2 * m > n[d] - 1)) b.full = 1;
+      if (sh[d][0] != INT_MAX) {
+        atomicMin(&gr->box[d], sh[d][0]);
+        atomicMax(&gr->box[3 + d], sh[3 + d][0]);
+      }
     }
-    bp->prev = bp->cur;
-    bp->cur = b;
+    __threadfence();
+    last = (atomicAdd(&gr->count[0], 1u) == gridDim.x - 1);
   }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; d++) {
+    lo[d] = atomicAdd(&gr->box[d], 0);
+    hi[d] = atomicAdd(&gr->box[3 + d], 0);
+    gr->box[d] = INT_MAX;
+    gr->box[3 + d] = INT_MIN;
+  }
+  gr->count[0] = 0u;
+  Box b;
+  b.full = 0;
+  b.empty = (lo[0] == INT_MAX);
+  const int n[3] = {a.nx, a.ny, a.nz};
+  for (int d = 0; d < 3; d++) {
+    b.lo[d] = b.empty ? 0 : lo[d] - iron;
+    b.hi[d] = b.empty ? -1 : hi[d] + iron;
+    if (!b.empty && (b.lo[d] - 2 * m < 0 || b.hi[d] + 2 * m > n[d] - 1)) b.full = 1;
+  }
+  bp->prev = bp->cur;
+  bp->cur = b;
 }
 
 // region of a box widened by e cells, or the whole grid; false if empty
@@ -243,7 +266,8 @@ int impurity_density(Handle *h) {
   const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
   const DepArgs d = dep_args(h);
   const unsigned gb = box_grid(h);
-  k_box_find<<<1, 1024, 0, h->stream>>>(h->rimp, d, h->p.ironx, h->st.m, h->box);
+  const unsigned pg = (unsigned)std::max(1, std::min(kPartMaxCta, (h->npar + kPartThreads - 1) / kPartThreads));
+  k_box_find<<<pg, kPartThreads, 0, h->stream>>>(h->rimp, d, h->p.ironx, h->st.m, h->gred, h->box);
   HE4_LAUNCHED(h);
   k_box_clear<<<gb, 256, 0, h->stream>>>(h->box, h->denx, h->psix, h->hpsix, h->counts, g, h->st.m);
   HE4_LAUNCHED(h);

@@ -32,6 +32,44 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return r;
 }
 
+// Grid-wide sums of NV values that stay deterministic on any number of
+// CTAs: every CTA reduces its values with block_sum and stores the results
+// as part[v * gridDim.x + blockIdx.x]; the CTA that finishes last (counted
+// on *counter) sums the partials of each value in index order with a fixed
+// thread assignment, so the totals do not depend on which CTA that is.
+// Returns true in the last CTA, whose thread 0 then holds the totals in
+// tot; the last CTA also resets *counter for the next launch.  All threads
+// of every CTA must call it.  `sh` holds blockDim/32 + 1 doubles.
+template <int NV>
+__device__ __forceinline__ bool grid_sums_last(const double (&v)[NV], double *part, unsigned *counter, double *sh,
+                                               double (&tot)[NV]) {
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+  const unsigned G = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    const double s = block_sum(v[i], sh);
+    if (tid == 0) part[(size_t)i * G + b] = s;
+  }
+  __shared__ int last;
+  if (tid == 0) {
+    __threadfence();  // this CTA's partials are visible before it is counted
+    last = (atomicAdd(counter, 1u) == G - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    double acc = 0.0;
+    for (unsigned c = tid; c < G; c += nthreads) acc += __ldcg(part + (size_t)i * G + c);
+    tot[i] = block_sum(acc, sh);
+  }
+  if (tid == 0) *counter = 0u;
+  return true;
+}
+
 // Reduce `nvals` independent partial arrays part[v*stride + b], b < nb, into
 // out[v] = (mult * sum_b part[...]) / div (one CTA of 1024 threads).
 __global__ void k_finalize_sums(const double *__restrict__ part, size_t stride, int nb, int nvals, double mult,

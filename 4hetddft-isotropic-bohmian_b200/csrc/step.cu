@@ -134,7 +134,10 @@ __global__ void k_den(const double2 *__restrict__ psi, double *den, size_t n) {
 }
 
 // ---------------------------------------------------------------------------
-// particles (one CTA; n3 = 3 N_par <= 3 * 2^20)
+// particles: elementwise over n3 = 3 N_par values on part_grid() CTAs; the
+// corrector errors and the means are grid-wide sums that stay deterministic
+// (grid_sums_last: fixed-order per-CTA partials, summed in index order by
+// the CTA that finishes last)
 // ---------------------------------------------------------------------------
 struct PartPtrs {
   double *rimp, *vimp, *aimp, *qr, *qv, *pcr, *pcv;
@@ -142,8 +145,13 @@ struct PartPtrs {
   int n3;
 };
 
+static unsigned part_grid(int n) {
+  return (unsigned)std::max(1, std::min(kPartMaxCta, (n + kPartThreads - 1) / kPartThreads));
+}
+
 // RK-Gill stage for positions and velocities (steprk.f90:236-260)
-__global__ void k_part_rk(PartPtrs P, double ar, double br, double cr, double dt, int first) {
+__global__ void __launch_bounds__(kPartThreads) k_part_rk(PartPtrs P, double ar, double br, double cr, double dt,
+                                                          int first) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.n3; t += gridDim.x * blockDim.x) {
     const double v = P.vimp[t];
     const double sr = ar * (v - br * P.qr[t]);
@@ -163,7 +171,7 @@ __global__ void k_part_rk(PartPtrs P, double ar, double br, double cr, double dt
 
 // predictor + modifier for positions and velocities (steppc.f90:68-85).
 // r1..r3 = rimpold(ioldr(1..3)) etc.
-__global__ void k_part_predict(PartPtrs P, double dt) {
+__global__ void __launch_bounds__(kPartThreads) k_part_predict(PartPtrs P, double dt) {
   const double c112 = 112.0 / 121.0, c4o3 = 4.0 / 3.0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.n3; t += gridDim.x * blockDim.x) {
     const double sr = P.r3[t] + c4o3 * dt * (2.0 * P.vimp[t] - P.v1[t] + 2.0 * P.v2[t]);
@@ -178,45 +186,54 @@ __global__ void k_part_predict(PartPtrs P, double dt) {
 }
 
 // corrector for positions and velocities (steppc.f90:126-147); out[0..1] =
-// errimp, errvimp.  Single CTA so the error sums are deterministic.
-__global__ void k_part_correct(PartPtrs P, double dt, double npar, double *out) {
-  __shared__ double sh[32];
+// errimp, errvimp (steppc.f90:136,147)
+__global__ void __launch_bounds__(kPartThreads) k_part_correct(PartPtrs P, double dt, double npar, GridRed *gr,
+                                                               double *out) {
+  __shared__ double sh[kPartThreads / 32 + 1];
   const double c9 = 9.0 / 121.0;
-  double er = 0.0, ev = 0.0;
-  for (int t = threadIdx.x; t < P.n3; t += blockDim.x) {
+  double e[2] = {0.0, 0.0};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.n3; t += gridDim.x * blockDim.x) {
     const double sr = 0.125 * (9.0 * P.r3[t] - P.r2[t] + 3.0 * dt * (P.v3[t] + 2.0 * P.vimp[t] - P.v1[t]));
     const double pr = P.pcr[t] - sr;
     P.pcr[t] = pr;
     P.rimp[t] = sr + c9 * pr;
-    er += fabs(c9 * pr);
+    e[0] += fabs(c9 * pr);
     // velocities use the pre-rotation ioldv slots (v2 = vimpold(ioldv(2)))
     const double sv = 0.125 * (9.0 * P.vimp[t] - P.v2[t] + 3.0 * dt * (P.aimp[t] + 2.0 * P.a1[t] - P.a2[t]));
     const double pv = P.pcv[t] - sv;
     P.pcv[t] = pv;
     P.v3[t] = P.vimp[t];
     P.vimp[t] = sv + c9 * pv;
-    ev += fabs(c9 * pv);
+    e[1] += fabs(c9 * pv);
   }
-  const double sr = block_sum(er, sh);
-  const double sv = block_sum(ev, sh);
-  if (threadIdx.x == 0) {
-    out[0] = sr * 0.3333333333 / npar;
-    out[1] = sv * 0.3333333333 / npar;
+  double tot[2];
+  if (grid_sums_last<2>(e, gr->part, &gr->count[1], sh, tot) && threadIdx.x == 0) {
+    out[0] = tot[0] * 0.3333333333 / npar;
+    out[1] = tot[1] * 0.3333333333 / npar;
   }
 }
 
-// means of rimp, vimp, aimp per axis (DFT4He3d.f90:864-878)
-__global__ void k_part_means(const double *__restrict__ rimp, const double *__restrict__ vimp,
-                             const double *__restrict__ aimp, int npar, double *out) {
-  __shared__ double sh[32];
-  const double *arr[3] = {rimp, vimp, aimp};
-  for (int a = 0; a < 3; a++)
+// means of rimp, vimp, aimp per axis (DFT4He3d.f90:864-878): out[a*3+c]
+__global__ void __launch_bounds__(kPartThreads) k_part_means(const double *__restrict__ rimp,
+                                                             const double *__restrict__ vimp,
+                                                             const double *__restrict__ aimp, int npar, GridRed *gr,
+                                                             double *out) {
+  __shared__ double sh[kPartThreads / 32 + 1];
+  double acc[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) acc[i] = 0.0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npar; p += gridDim.x * blockDim.x) {
+#pragma unroll
     for (int c = 0; c < 3; c++) {
-      double acc = 0.0;
-      for (int p = threadIdx.x; p < npar; p += blockDim.x) acc += arr[a][c * npar + p];
-      const double s = block_sum(acc, sh);
-      if (threadIdx.x == 0) out[a * 3 + c] = s / npar;
+      acc[c] += rimp[c * npar + p];
+      acc[3 + c] += vimp[c * npar + p];
+      acc[6 + c] += aimp[c * npar + p];
     }
+  }
+  double tot[9];
+  if (grid_sums_last<9>(acc, gr->part, &gr->count[2], sh, tot) && threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 9; i++) out[i] = tot[i] / npar;
 }
 
 // ---------------------------------------------------------------------------
@@ -279,7 +296,8 @@ int field_split_fields(Handle *h) {
 }
 
 int particle_means(Handle *h, double *dmeans) {
-  k_part_means<<<1, 1024, 0, h->stream>>>(h->rimp, h->vimp, h->aimp, h->npar, dmeans);
+  k_part_means<<<part_grid(h->npar), kPartThreads, 0, h->stream>>>(h->rimp, h->vimp, h->aimp, h->npar, h->gred,
+                                                                   dmeans);
   HE4_LAUNCHED(h);
   return HE4_OK;
 }
@@ -325,7 +343,8 @@ int step_rk(Handle *h, double dt, double *dres) {
     // ring indices are the identity during the starter
     for (int i = 0; i < 3; i++) h->ioldr[i] = h->ioldv[i] = h->ioldp[i] = i;
     for (int i = 0; i < 2; i++) h->iolda[i] = h->ioldh[i] = i;
-    k_part_rk<<<1, 1024, 0, h->stream>>>(part_ptrs(h), arun[jr], brun[jr], crun[jr], dt, jr == 0);
+    k_part_rk<<<part_grid(3 * h->npar), kPartThreads, 0, h->stream>>>(part_ptrs(h), arun[jr], brun[jr], crun[jr],
+                                                                       dt, jr == 0);
     HE4_LAUNCHED(h);
     if (jr <= 2) HE4_TRY(field_all(h));
   }
@@ -354,7 +373,7 @@ int step_pc(Handle *h, double dt, double *dres) {
     std::swap(h->ioldh[0], h->ioldh[1]);
   }
   // particles
-  k_part_predict<<<1, 1024, 0, h->stream>>>(part_ptrs(h), dt);
+  k_part_predict<<<part_grid(3 * h->npar), kPartThreads, 0, h->stream>>>(part_ptrs(h), dt);
   HE4_LAUNCHED(h);
   std::swap(h->iolda[0], h->iolda[1]);
   HE4_TRY(field_all(h));
@@ -380,7 +399,8 @@ int step_pc(Handle *h, double dt, double *dres) {
     HE4_LAUNCHED(h);
   }
   // particles corrector (uses the pre-rotation ring indices), then rotations
-  k_part_correct<<<1, 1024, 0, h->stream>>>(part_ptrs(h), dt, (double)h->npar, dres + 1);
+  k_part_correct<<<part_grid(3 * h->npar), kPartThreads, 0, h->stream>>>(part_ptrs(h), dt, (double)h->npar,
+                                                                           h->gred, dres + 1);
   HE4_LAUNCHED(h);
   rot3(h->ioldr);
   rot3(h->ioldv);

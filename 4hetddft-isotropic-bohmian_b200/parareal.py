@@ -288,8 +288,10 @@ class Parareal:
     def run(self, psi0, r0, v0, tol=1e-6, max_iter=None, fallback=True, contraction=0.5, first_change_max=0.1,
             judge_first=True, judge_max=None, log=None):
         """Returns a dict: iterations, per-iteration max relative psi change,
-        wall seconds (device-synchronised), fine steps executed, and where the
-        sequential fallback took over.  fallback: when an iteration does not
+        wall seconds (device-synchronised), fine steps executed, whether the
+        iteration converged (change <= tol), and where the sequential
+        fallback took over (exact_by_fallback: the result is the sequential
+        fine solution because the fallback ran).  fallback: when an iteration does not
         shrink the change by `contraction`, or a fine run leaves the range
         the solver integrates, the remaining slices are integrated one after
         the other from the last exact boundary (the plain integrator is both
@@ -387,7 +389,11 @@ class Parareal:
         ev1.synchronize()
         wall = time.perf_counter() - t0
         device_s = ev0.elapsed_time(ev1) * 1e-3
-        return {"iterations": k, "converged": converged or fallback_at is not None, "diverged": diverged,
+        # converged: the iteration itself met tol.  A run that fell back to
+        # the sequential integrator also ends on the exact fine solution,
+        # but did not converge; exact_by_fallback says so.
+        return {"iterations": k, "converged": converged, "exact_by_fallback": fallback_at is not None,
+                "diverged": diverged,
                 "fallback_at": fallback_at, "changes": history, "wall_s": wall, "device_s": device_s,
                 "fine_steps": self.fine_steps}
 

@@ -7,8 +7,8 @@
  * per-time-step calls of its main loop with explicit entry points on a handle
  * that owns every device array.  The Fortran host keeps the namelist parsing
  * (DFT4He3d.f90:147-187), readenc/printoutc file I/O and diagnostics and binds
- * these functions through ISO_C_BINDING (see INTEGRATION.md for the interface
- * block).
+ * these functions through an ISO_C_BINDING interface block, one bind(C)
+ * interface per entry point below.
  *
  * Conventions
  *  - Grid arrays are x-fastest: C [nz][ny][nx] == Fortran a(nx,ny,nz).
@@ -199,9 +199,11 @@ int he4_bubble_radius(he4_handle *h, int32_t nr, double *rb, int32_t found[2],
  * (four partial sums per z plane), so nz may not exceed 4096: larger grids
  * return HE4_E_ARG.  The first call on a device looks up that array's
  * device address (cudaGetSymbolAddress, with the device current); make
- * that first call before any stream capture.  All calls share the array:
- * calls that may overlap on the GPU (other streams, other threads) race and
- * must be serialised by the caller. */
+ * that first call before any stream capture.  The address stays cached for
+ * the life of the process; after cudaDeviceReset on that device it is stale,
+ * so do not call this function on a device the host has reset.  All calls
+ * share the array: calls that may overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller. */
 int he4_diagnostics_noalloc(const double *den, int32_t nx, int32_t ny, int32_t nz,
                             double xmax, double ymax, double zmax, int32_t n4,
                             double *out, void *stream);
@@ -237,11 +239,13 @@ int he4_fft_c2r(he4_handle *h, const double *in, double *out);
  * which: 0 z-pass convolution (FFT_z, kernel multiply, IFFT_z), 1 y pass,
  * 2 x pass R2C, 3 x pass C2R, 4 plain z pass, 5 z convolution without a
  * kernel, 6 z convolution with three outputs (these only touch FFT scratch
- * buffers), 7 the density gradient stencil, 8 the merged pot4 assembly
- * (these rewrite fields of the current evaluation with the same values, so
- * call them after a field evaluation).  Returns
- * the mean time per launch, the algorithmic bytes one launch moves (each
- * input read once, each output written once) and the kernel's name. */
+ * buffers), 7 the density gradient stencil, 8 the merged pot4 assembly on
+ * FP64 grids, 9 the merged pot4 assembly on the float grids of the
+ * FP32-convolution form, 10 the x pass C2R into a float grid (9 and 10
+ * need that form; 7-10 rewrite fields of the current evaluation, so call
+ * them after a field evaluation; the next step evaluates its field again).
+ * Returns the mean time per launch, the algorithmic bytes one launch moves
+ * (each input read once, each output written once) and the kernel's name. */
 int he4_bench_kernel(he4_handle *h, int32_t which, int32_t reps, double *ms_per_launch,
                      double *bytes_per_launch, char *name, int32_t name_len);
 

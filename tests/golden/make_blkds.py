@@ -87,7 +87,13 @@ def centre_row(A, M, K):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/mates.f"
+    if len(sys.argv) > 1:
+        src = sys.argv[1]
+    elif os.environ.get("HE4_REFERENCE_DIR"):
+        src = os.path.join(os.environ["HE4_REFERENCE_DIR"], "mates.f")
+    else:
+        sys.exit("usage: make_blkds.py <path of the reference's mates.f> "
+                 "(or set HE4_REFERENCE_DIR to the reference checkout)")
     A = parse_table(src)
     out = {}
     for M in range(3, 26, 2):
