@@ -199,24 +199,36 @@ def gpu_arm(args):
     forms = {}
     sim_ps = args.steps * DT_FS * 1e-3
     step_form = "fp32" if args.form == "parareal" else args.form
+    g = stream = None
     for form in ("fp64", "fp32"):
         if form != step_form and not args.all_forms:
             continue
         gf = pkg.He4Step(form_params(pkg, p, form))
         sf = torch.cuda.ExternalStream(gf.stream(), device=torch.device("cuda", local))
         ms_f, launches_f, clocks_f = timed_run(gf, sf)
-        forms[form] = {"form": FORMS[form], "ms_per_step": ms_f / args.steps,
+        ms_step = ms_f / args.steps
+        forms[form] = {"form": FORMS[form], "ms_per_step": ms_step,
                        "value": replica_throughput(world, sim_ps, ms_f * 1e-3), "gpu_launches": launches_f,
                        "clocks": clocks_f}
+        # whole-step roofline: the algorithmic bytes of one PC step over its time
+        peak, _ = load_peaks()
+        sb = step_bytes(form, p.nx * p.ny * p.nz)
+        forms[form]["step_roofline"] = {"bytes_per_step": sb, "achieved_gbs": sb / (ms_step * 1e-3) / 1e9,
+                                        "peak_gbs": peak, "frac": sb / (ms_step * 1e-3) / 1e9 / peak}
+        forms[form]["roofline"] = kernel_roofline(pkg, gf, args, form)
+        forms[form]["e2e"] = e2e_leg(pkg, torch, gf, psi, r, v, dt, args, barrier, dist, local, world)
         if form == step_form:
             g, stream = gf, sf
             ms_max, launches, clocks = ms_f, launches_f, clocks_f
         else:
             gf.close()
     value = replica_throughput(world, sim_ps, ms_max * 1e-3)
-
-    # ---- dominant-kernel roofline, measured live with CUDA events
-    roof = kernel_roofline(pkg, g, stream, args, step_form)
+    roof = dict(forms[step_form]["roofline"] or {})
+    if roof:
+        roof["step_frac"] = forms[step_form]["step_roofline"]["frac"]
+        roof["step_bytes"] = forms[step_form]["step_roofline"]["bytes_per_step"]
+        roof["form"] = step_form
+    e2e = forms[step_form]["e2e"]
 
     par = None
     if args.form == "parareal":
@@ -225,52 +237,22 @@ def gpu_arm(args):
         par["e2e_s"] = max_over_ranks(dist, par["e2e_s"], f"cuda:{local}")
         par["value"] = replica_throughput(world, par["sim_ps"], dev_s)
         par["ms_per_step"] = dev_s * 1e3 / (PARAREAL_SLICES * PARAREAL_STEPS)
+        nsteps_par = PARAREAL_SLICES * PARAREAL_STEPS
+        # end to end = the parareal run from host buffers to the final state
+        # on the host (initial upload, training excluded, final download)
+        par["e2e"] = {"value": replica_throughput(world, par["sim_ps"], par["e2e_s"]), "unit": "simulated ps/hour",
+                      "h2d_bytes_per_step": par["e2e_h2d"] / nsteps_par,
+                      "d2h_bytes_per_step": par["e2e_d2h"] / nsteps_par, "steps": nsteps_par,
+                      "includes": "parareal run from host state: upload, iterations, fallback, final-state download"}
         forms["parareal"] = par
         value = par["value"]
         ms_max = par["ms_per_step"]
         launches = par["gpu_launches"]
         clocks = par["clocks"]
+        e2e = par["e2e"]
 
     if args.ensemble > 0 and world == 1:
         forms["ensemble"] = ensemble_form(pkg, args, local, barrier)
-
-    # ---- end to end through the per-step C ABI with host buffers:
-    # he4_set_state (pinned host -> device), 3 he4_step_rk + (K-3)
-    # he4_step_pc (each returns err/means to the host), he4_get_state.
-    psi_h = pin(torch, psi.view(np.float64))
-    r_h, v_h = pin(torch, r), pin(torch, v)
-    out_psi = pin(torch, np.zeros_like(psi).view(np.float64))
-    out_r = pin(torch, np.zeros_like(r))
-    L = pkg.load_library()
-    dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_double))
-    e2e_steps = max(args.steps, 4)
-    e_buf, m_buf = (C.c_double * 3)(), (C.c_double * 9)()
-    barrier()
-    t0 = time.perf_counter()
-    assert L.he4_set_state(g._h, dp(psi_h), dp(r_h), dp(v_h)) == 0
-    for s in range(e2e_steps):
-        if s < 3:
-            rc = L.he4_step_rk(g._h, dt, m_buf)
-        else:
-            rc = L.he4_step_pc(g._h, dt, e_buf, m_buf)
-        if rc != 0:
-            raise RuntimeError(f"step failed: {rc}")
-    assert L.he4_get_state(g._h, dp(out_psi), dp(out_r), None, None) == 0
-    t1 = time.perf_counter()
-    e2e_s = max_over_ranks(dist, t1 - t0, f"cuda:{local}")
-    h2d = psi.nbytes + r.nbytes + v.nbytes
-    d2h = psi.nbytes + r.nbytes + (3 * 8 + 9 * 8) * (e2e_steps - 3) + 9 * 8 * 3
-    e2e_value = replica_throughput(world, e2e_steps * DT_FS * 1e-3, e2e_s)
-
-    if par is not None:
-        # end to end = the parareal run from host buffers to the final state
-        # on the host (initial upload, training excluded, final download)
-        e2e_value = replica_throughput(world, par["sim_ps"], par["e2e_s"])
-        h2d, d2h = par["e2e_h2d"], par["e2e_d2h"]
-        e2e_steps = PARAREAL_SLICES * PARAREAL_STEPS
-        e2e_note = "parareal run from host state: upload, iterations, fallback, final-state download"
-    else:
-        e2e_note = "3 RK-Gill starter steps, per-step err/means copy-out, state upload and download"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -281,6 +263,9 @@ def gpu_arm(args):
         dist.destroy_process_group()
     if rank != 0:
         return
+    timed = ("K predictor-corrector steps from device-resident state (he4_run); K = --steps" if par is None else
+             f"a fixed {PARAREAL_SLICES} x {PARAREAL_STEPS} fs of parareal from device-resident state (FNO "
+             f"training untimed); --steps K sets the K PC steps each step form in 'forms' times")
     line = {
         "metric": METRIC,
         "value": value,
@@ -302,14 +287,11 @@ def gpu_arm(args):
             "form": FORMS[args.form],
             "parallelism": f"replicas x{world} (no data-path collective)",
             "l2": "inputs larger than L2: every grid array is >= 134 MB",
-            "timed": ("K predictor-corrector steps from device-resident state (he4_run)" if par is None else
-                      f"{PARAREAL_SLICES} x {PARAREAL_STEPS} fs of parareal from device-resident state "
-                      "(FNO training untimed)"),
+            "timed": timed,
         },
-        "e2e": {"value": e2e_value, "unit": "simulated ps/hour", "h2d_bytes_per_step": h2d / e2e_steps,
-                "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps, "includes": e2e_note},
+        "e2e": e2e,
         "gpu_launches": launches,
-        "roofline": roof,
+        "roofline": roof or None,
         "clocks": clocks,
         "forms": forms,
     }
@@ -323,9 +305,11 @@ def gpu_arm(args):
 def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     """Train the FNO coarse propagator on solver trajectories of the 128^3
     family (FP32 form, restricted to 64^3), then run parareal on the
-    workload: 16 slices of 50 fine steps, FP32-convolution fine propagator.
-    The timed region is the parareal run; its final state is compared with
-    the plain FP64 sequential run over the same 800 fs."""
+    workload: PARAREAL_SLICES slices of PARAREAL_STEPS fine steps (6 x 50 fs:
+    the 256^3 workload leaves the range the integrator handles after about
+    300 fs), FP32-convolution fine propagator.  The timed region is the
+    parareal run; its final state is compared with the plain FP64
+    sequential run over the same 300 fs."""
     import torch
     w, pr, fno = pkg.workloads, pkg.parareal, pkg.fno
     dev = torch.device("cuda", local)
@@ -375,7 +359,8 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     sim_ps = S * K * DT_FS * 1e-3
     return {"form": FORMS["parareal"], "sim_ps": sim_ps, "device_s": res["device_s"], "e2e_s": e2e_s,
             "iterations": res["iterations"],
-            "converged": res["converged"], "diverged": res["diverged"], "fallback_at": res["fallback_at"],
+            "converged": res["converged"], "exact_by_fallback": res["exact_by_fallback"],
+            "diverged": res["diverged"], "fallback_at": res["fallback_at"],
             "changes": res["changes"], "fine_steps_executed": res["fine_steps"],
             "fno": {"training_trajectories": args.fno_traj, "training_steps": args.fno_steps,
                     "held_out_rel_error_before": before, "held_out_rel_error_after": after,
@@ -453,34 +438,84 @@ def pin(torch, a):
     return t
 
 
-def kernel_roofline(pkg, g, stream, args, form):
-    """Average duration of the dominant kernel, timed with CUDA events on the
-    library's stream, against its algorithmic bytes."""
+# dominant kernel of each step form's launch list (profiles/launch_list_*):
+# he4_bench_kernel ids 9 (merged pot4 on float grids) and 3 (x pass C2R)
+DOMINANT_KERNEL = {"fp32": 9, "fp64": 3}
+
+
+def step_bytes(form, n):
+    """Algorithmic bytes of one PC step of an n-point grid: every pointwise
+    op fused into an adjacent FFT or stencil pass, each FFT one read and one
+    write, each kernel array read once per use, stencils reading their
+    inputs once (R = 8n bytes a real grid, a half spectrum S ~ R).  Per
+    field evaluation 60R + 28S (forward FFTs 18R + 10S, inverse 18S + 12R,
+    stencils and pointwise ~30R), per step two evaluations plus 39R of
+    predictor / corrector: 215R = 1720 n bytes.  The FP32-convolution form
+    halves the FFT and convolution bytes: per evaluation 45R + 14S, per step
+    157R = 1256 n bytes."""
+    return (1256 if form == "fp32" else 1720) * float(n)
+
+
+def kernel_roofline(pkg, g, args, form, reps=20):
+    """Average duration of the form's dominant kernel, timed with CUDA
+    events on the library's stream (the kernel's own launch stream), against
+    its algorithmic bytes; DRAM traffic per launch from the committed ncu
+    capture of the same kernel."""
     L = pkg.load_library()
-    if not hasattr(L, "he4_bench_kernel"):
-        return None
     L.he4_bench_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double), C.c_char_p, C.c_int32]
     ms, byts = C.c_double(), C.c_double()
     name = C.create_string_buffer(64)
-    rc = L.he4_bench_kernel(g._h, 0, 20, C.byref(ms), C.byref(byts), name, 64)
+    which = DOMINANT_KERNEL[form]
+    g.field()  # the stencil ids work on the fields of a current evaluation
+    rc = L.he4_bench_kernel(g._h, which, reps, C.byref(ms), C.byref(byts), name, 64)
     if rc != 0:
         return None
     peak, src = load_peaks()
     achieved = byts.value / (ms.value * 1e-3) / 1e9
     kname = name.value.decode()
-    # DRAM bytes per launch of this kernel from the committed ncu capture of
-    # the same launch at 256^3 (profiles/fft_passes_c3.md)
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "fft_passes_c3.json")
+    traffic, tsrc = None, None
+    prof = os.path.join(ROOT, "profiles", "dominant_kernels_traffic.json")
     if args.config == "c3" and os.path.exists(prof):
-        key = kname if form == "fp64" else f"{kname}:{form}"
-        traffic = json.load(open(prof))["traffic_bytes_per_launch"].get(key)
-    return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
+        ent = json.load(open(prof))["kernels"].get(f"{form}:{which}")
+        if ent:
+            traffic, tsrc = ent["traffic_bytes_per_launch_256"], ent["source"]
+    return {"kernel": kname, "bench_id": which, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src,
-            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-            "traffic_source": "ncu dram__bytes, profiles/fft_passes_c3.md" if traffic else None,
-            "bytes_per_launch": byts.value, "ms_per_launch": ms.value}
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "traffic_source": tsrc,
+            "bytes_per_launch": byts.value, "ms_per_launch": ms.value, "launches_timed": reps}
+
+
+def e2e_leg(pkg, torch, g, psi, r, v, dt, args, barrier, dist, local, world):
+    """The same metric end to end through the per-step C ABI with host
+    buffers: he4_set_state (pinned host -> device), 3 he4_step_rk + (K-3)
+    he4_step_pc (each returns its errors and means to the host),
+    he4_get_state (device -> pinned host)."""
+    psi_h = pin(torch, psi.view(np.float64))
+    r_h, v_h = pin(torch, r), pin(torch, v)
+    out_psi = pin(torch, np.zeros_like(psi).view(np.float64))
+    out_r = pin(torch, np.zeros_like(r))
+    L = pkg.load_library()
+    dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_double))
+    steps = max(args.steps, 4)
+    e_buf, m_buf = (C.c_double * 3)(), (C.c_double * 9)()
+    barrier()
+    t0 = time.perf_counter()
+    if L.he4_set_state(g._h, dp(psi_h), dp(r_h), dp(v_h)) != 0:
+        raise RuntimeError("he4_set_state failed")
+    for s in range(steps):
+        rc = L.he4_step_rk(g._h, dt, m_buf) if s < 3 else L.he4_step_pc(g._h, dt, e_buf, m_buf)
+        if rc != 0:
+            raise RuntimeError(f"step failed: {rc}")
+    if L.he4_get_state(g._h, dp(out_psi), dp(out_r), None, None) != 0:
+        raise RuntimeError("he4_get_state failed")
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(dist, t1 - t0, f"cuda:{local}")
+    h2d = psi.nbytes + r.nbytes + v.nbytes
+    d2h = psi.nbytes + r.nbytes + (3 * 8 + 9 * 8) * (steps - 3) + 9 * 8 * 3
+    return {"value": replica_throughput(world, steps * DT_FS * 1e-3, e2e_s), "unit": "simulated ps/hour",
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps, "steps": steps,
+            "includes": "3 RK-Gill starter steps, per-step err/means copy-out, state upload and download"}
 
 
 def cpu_baseline(pkg, args, target_s=20.0):
@@ -549,27 +584,33 @@ def reference_arm(args):
         "dtype": "f64",
         "data": "synthetic (Fermi-profile droplet, seeded Gaussian test particles)",
         "config": {"workload": f"{args.config}: {cfg['n']}^3 grid, N={cfg['n4']} He, {cfg['npar']} test "
-                               f"particles, core4=OTC npd=7, plain FP64 predictor-corrector steps"},
+                               f"particles, core4=OTC npd=7, plain FP64 predictor-corrector steps",
+                   "timed": f"min(K, 3) = {steps} PC steps after {warm} untimed: a bounded sample of the CPU run "
+                            "(about 1.7 s per step on 16 threads at 256^3); simulated ps/hour is a rate, so "
+                            "the sample length does not change it"},
         "cpu_baseline": {"value": value, "unit": "simulated ps/hour", "cores": threads, "kind": "port",
                          "sample": f"{steps} PC steps (bounded sample of the {args.config} workload)"},
         "e2e": {"value": value, "unit": "simulated ps/hour", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
-def profile_kernels(form):
-    """One field evaluation of the 256^3 workload, then one warm-up and one
-    timed launch of each pass he4_bench_kernel measures: the workload the
-    ncu summaries under profiles/ capture (profiles/fft_passes_c3.md)."""
+def profile_kernels(form, config="c3"):
+    """One field evaluation of a workload, then one warm-up and one timed
+    launch of each pass he4_bench_kernel measures: the workload the ncu
+    summaries under profiles/ capture (the 128^3 config keeps a capture at
+    a few GB on the device)."""
     pkg = load_pkg()
     w = pkg.workloads
-    p, psi, r, v, _ = w.workload("c3")
+    p, psi, r, v, _ = w.workload(config)
     g = pkg.He4Step(form_params(pkg, p, form))
     g.set_state(psi, r, v)
     g.field()
     L = pkg.load_library()
     L.he4_bench_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double), C.c_char_p, C.c_int32]
-    for which in (0, 1, 2, 3, 6, 7, 8):
+    ids = (0, 1, 2, 3, 6, 7, 8) + ((9, 10) if form == "fp32" else ())
+    for which in ids:
+        g.field()
         ms, b = C.c_double(), C.c_double()
         nm = C.create_string_buffer(64)
         if L.he4_bench_kernel(g._h, which, 1, C.byref(ms), C.byref(b), nm, 64) != 0:
@@ -595,10 +636,10 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-kernels", choices=["fp64", "fp32"], default=None,
-                    help="run each FFT/stencil pass once on the 256^3 workload (for ncu captures) and exit")
+                    help="run each FFT/stencil pass once on the --config workload (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_kernels:
-        profile_kernels(args.profile_kernels)
+        profile_kernels(args.profile_kernels, args.config)
         return
     if args.warmup < 3:
         args.warmup = 3
