@@ -134,6 +134,12 @@ static int create(const he4_params *pin, Handle *h) {
     return HE4_E_ARG;
   }
   h->dev = pin->device;
+  // HE4_STREAM_STENCILS=0 selects the register z-marching stencils instead of
+  // the bulk-copy streamed ones (same results to rounding; for comparisons)
+  {
+    const char *s = getenv("HE4_STREAM_STENCILS");
+    h->use_stream = (s && s[0] == '0') ? 0 : 1;
+  }
   HE4_CUDA_TRY(cudaSetDevice(h->dev));
   cudaDeviceProp prop;
   HE4_CUDA_TRY(cudaGetDeviceProperties(&prop, h->dev));
@@ -423,9 +429,30 @@ int he4_snapshot_wait(he4_handle *hh, const double **psi, const double **rimp, c
   return HE4_OK;
 }
 
+}  // extern "C"
+
+namespace he4 {
+int check_kernel_errors(Handle *h) {
+  unsigned *herr = reinterpret_cast<unsigned *>(h->hscal + 60);
+  HE4_CUDA_TRY(cudaMemcpyAsync(herr, &h->gred->err, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (*herr) {
+    const unsigned e = *herr;
+    *herr = 0;
+    HE4_CUDA_TRY(cudaMemsetAsync(&h->gred->err, 0, sizeof(unsigned), h->stream));
+    HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    set_error("a streamed stencil's bulk copies did not arrive within one second (device error word 0x%x)", e);
+    return HE4_E_CUDA;
+  }
+  return HE4_OK;
+}
+}  // namespace he4
+
+extern "C" {
+
 static int sync_and_check(Handle *h) {
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return HE4_OK;
+  return check_kernel_errors(h);
 }
 
 int he4_potenimp(he4_handle *hh) {
@@ -477,6 +504,7 @@ int he4_step_rk(he4_handle *hh, double deltat, double means[9]) {
   HE4_TRY(step_rk(h, deltat, h->scal));
   HE4_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  HE4_TRY(check_kernel_errors(h));
   if (means) memcpy(means, h->hscal + 3, 9 * sizeof(double));
   if (!finite_all(h->hscal, 12)) {
     set_error("non-finite trajectory means after steprk");
@@ -495,6 +523,7 @@ int he4_step_pc(he4_handle *hh, double deltat, double err[3], double means[9]) {
   HE4_TRY(step_pc(h, deltat, h->scal));
   HE4_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  HE4_TRY(check_kernel_errors(h));
   if (err) memcpy(err, h->hscal, 3 * sizeof(double));
   if (means) memcpy(means, h->hscal + 3, 9 * sizeof(double));
   if (!finite_all(h->hscal, 12)) {
@@ -535,6 +564,7 @@ int he4_run(he4_handle *hh, int32_t nsteps, double deltat, double *err, double *
     }
   }
   cudaFreeAsync(dres, h->stream);
+  if (e == HE4_OK) e = check_kernel_errors(h);
   if (e == HE4_OK) {
     for (int s = 0; s < nsteps; s++) {
       if (err) memcpy(err + 3 * s, hres + 12 * s, 3 * sizeof(double));
@@ -712,7 +742,7 @@ int he4_fft_c2r(he4_handle *hh, const double *in, double *out) {
   return HE4_OK;
 }
 
-constexpr int kBenchKernels = 11;
+constexpr int kBenchKernels = 12;
 
 static int launch_bench(Handle *h, int which) {
   switch (which) {
@@ -741,6 +771,7 @@ static int launch_bench(Handle *h, int which) {
     case 8: return launch_pot4_merged(h);
     case 9: return launch_pot4_merged_f32(h);
     case 10: return fft_x_c2r_f32_only(h, h->spec[1], h->g32[8]);
+    case 11: return launch_grad_f32(h);
     default: set_error("unknown kernel id %d", which); return HE4_E_ARG;
   }
 }
@@ -758,7 +789,8 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
       "k_zconv (z conv, 1 output)", "k_yz_pipe (y pass)",           "k_xr2c_reg (x R2C)",
       "k_xc2r_reg (x C2R)",         "k_zconv (z pass, no multiply)", "k_zconv (z conv, no kernel)",
       "k_zconv (z conv, 3 outputs)", "k_grad_z (density gradient)",  "k_pot4_merged_z (pot4, FP64 grids)",
-      "k_pot4_merged_z (pot4, float grids)", "k_xc2r_reg (x C2R, float rows)"};
+      "k_pot4_merged_z (pot4, float grids)", "k_xc2r_reg (x C2R, float rows)",
+      "k_grad_z (density gradient, float grids)"};
   const double H = (double)h->H, N = (double)h->N;
   // algorithmic bytes: read input once, write output once (+ the real
   // kernel); c and k are the sizes of a spectrum and a kernel element
@@ -771,12 +803,14 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
       // float grids: lin, dencg, h0..h2 (4 B), den in and pot4 out (8 B)
       5 * 4 * N + 2 * 8 * N,
       // half spectrum in, float rows out
-      c * H + 4 * N};
+      c * H + 4 * N,
+      // den in, three float gradients out
+      8 * N + 3 * 4 * N};
   if (which < 0 || which >= kBenchKernels) {
     set_error("unknown kernel id %d", which);
     return HE4_E_ARG;
   }
-  if ((which == 9 || which == 10) && !h->real32) {
+  if ((which == 9 || which == 10 || which == 11) && !h->real32) {
     set_error("kernel id %d needs the FP32-convolution form with float grids", which);
     return HE4_E_STATE;
   }

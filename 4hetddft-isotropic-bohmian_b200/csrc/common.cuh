@@ -123,6 +123,7 @@ struct GridRed {
   double part[9 * kPartMaxCta];
   unsigned count[4];  // 0: box, 1: corrector errors, 2: means
   int box[6];         // min x, y, z, max x, y, z; reset by the last CTA
+  unsigned err;       // bit 0: a streamed stencil's copies did not arrive
 };
 
 // ---------------------------------------------------------------------------
@@ -233,6 +234,8 @@ struct Handle {
   // captured PC steps (one per distinct StepState; the states repeat)
   std::vector<StepGraph> graphs;
   int use_graphs = 1;
+  // row-streamed (bulk-copy pipelined) stencils where the grid allows them
+  int use_stream = 1;
 };
 
 // kernel-level entry points used by the ABI layer
@@ -321,6 +324,10 @@ int launch_grad(Handle *h);
 bool real32_ok(const Handle *h);
 int launch_pot4_merged(Handle *h);
 int launch_pot4_merged_f32(Handle *h);
+int launch_grad_f32(Handle *h);
+// device error word of the step's kernels (GridRed::err): HE4_E_CUDA with a
+// message when set, after which it is cleared; synchronises the stream
+int check_kernel_errors(Handle *h);
 // potenimp + poten + forceimp; marks the fields valid.  split = false takes
 // the merged form when the z length allows it.
 int field_all(Handle *h, bool split = false);

@@ -6,6 +6,10 @@
 // transform) for the whole evaluation; forceimp reuses it, since for the
 // periodic stencils (icon=8) FFT(d_i rho) = i D_i(k) FFT(rho) exactly, D_i
 // being the symbol of the npd-point first-derivative stencil.
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "common.cuh"
 #include "stencil.cuh"
 
@@ -34,6 +38,9 @@ constexpr int kZBg = 4;  // planes per CTA of the gradient stencil
 struct OtArgs {
   double cp4, cpp4, den0s, h2o2m4, alphas, c_solid, beta, den_m;
 };
+}  // namespace he4
+#include "stream_stencil.cuh"
+namespace he4 {
 
 // periodic index for i in [-n, 2n)
 __device__ __forceinline__ int wrap2(int i, int n) { return i < 0 ? i + n : (i >= n ? (i >= 2 * n ? i - 2 * n : i - n) : i); }
@@ -429,7 +436,180 @@ static bool zmarch_ok(const Handle *h) {
 
 static dim3 grid_z(const Geo &g, int zb = kZB) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + zb - 1) / zb); }
 
+// ---------------------------------------------------------------------------
+// streamed stencils (stream_stencil.cuh): launch shapes and per-device
+// launch attributes
+// ---------------------------------------------------------------------------
+#ifndef HE4_STREAM_TY
+#define HE4_STREAM_TY 4
+#endif
+#ifndef HE4_STREAM_S
+#define HE4_STREAM_S 2
+#endif
+// Rows per CTA and planes in flight.  Measured at 256^3 (float grids,
+// CUDA events, 20 launches): TY 4 / S 2 gives pot4 206 us and the gradient
+// 143 us against 274 / 153 us for the register z-marching kernels; TY 2 /
+// S 3, TY 2 / S 4 and TY 4 / S 3 were slower.  On FP64 grids the register
+// kernels stay faster (pot4 247 vs 316 us, gradient 130 vs 139 us), so the
+// streamed kernels serve the float grids of the FP32-convolution form.
+constexpr int kStreamTY = HE4_STREAM_TY;
+constexpr int kStreamS = HE4_STREAM_S;
+
+// z planes per CTA: the chunk length whose grid fills the resident CTA
+// slots best (fewest waves on a tie), at least 8 planes per chunk
+static int stream_chunk(int nz, int ytiles, int resident) {
+  int best_zc = nz;
+  double best = -1.0;
+  for (int w = 1; w <= 8; w++) {
+    int nch = std::min(nz, (w * resident) / ytiles);
+    if (nch < 1) continue;
+    const int zc = (nz + nch - 1) / nch;
+    if (zc < 8 && nch > 1) continue;
+    const long ctas = (long)ytiles * ((nz + zc - 1) / zc);
+    const long waves = (ctas + resident - 1) / resident;
+    const double eff = (double)ctas / (double)(waves * resident);
+    if (eff > best + 1e-9) {
+      best = eff;
+      best_zc = zc;
+    }
+  }
+  return best_zc;
+}
+
+// resident CTAs of a streamed kernel on the handle's device, with its
+// dynamic shared memory limit raised there once (0: does not fit)
+template <typename K>
+static int stream_resident(const Handle *h, K kern, size_t smem) {
+  // per (kernel, device): the dynamic shared memory limit set so far, and
+  // the resident CTAs per shared memory size
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> limit;
+  static std::map<std::pair<std::pair<const void *, int>, size_t>, int> res;
+  if (smem > 227 * 1024) return 0;
+  const std::pair<const void *, int> key((const void *)kern, h->dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = res.find({key, smem});
+  if (it != res.end()) return it->second;
+  if (limit[key] < smem) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    limit[key] = smem;
+  }
+  int nsm = 0, occ = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem) != cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  res[{key, smem}] = occ * nsm;
+  return occ * nsm;
+}
+
+// the row-streamed kernels take periodic grids with 64, 128, 256 or 512
+// points along x (a template parameter of the kernels) and a y extent the
+// CTA rows divide; the shared memory fit is checked per launch
+static bool stream_ok(const Handle *h) {
+  return h->p.icon == 8 && (h->st.m == 3 || h->st.m == 6) &&
+         (h->nx == 64 || h->nx == 128 || h->nx == 256 || h->nx == 512) && h->ny % kStreamTY == 0 &&
+         h->ny >= 2 * h->st.m && h->nz >= 2 * h->st.m + 1;
+}
+
+template <typename TI, bool OTC, int M, int NX>
+static bool launch_pot4_stream(Handle *h, const TI *lin, const TI *dcg, const TI *h0, const TI *h1, const TI *h2,
+                               const OtArgs &ot) {
+  using L = Pot4StreamLayout<TI, OTC, M, kStreamTY, kStreamS, NX>;
+  auto kern = k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX>;
+  const int res = stream_resident(h, kern, L::total);
+  if (res == 0) return false;
+  const Geo g = geo(h);
+  const int yt = h->ny / kStreamTY, zc = stream_chunk(h->nz, yt, res);
+  kern<<<dim3(yt, (h->nz + zc - 1) / zc), 256, L::total, h->stream>>>(lin, h->den, dcg, h0, h1, h2, h->pot4, h->st, g,
+                                                                     ot, zc, &h->gred->err);
+  HE4_LAUNCHED(h);
+  return true;
+}
+
+template <typename TO, int M, int NX>
+static bool launch_grad_stream(Handle *h, TO *dx, TO *dy, TO *dz) {
+  using L = GradStreamLayout<TO, M, kStreamTY, kStreamS, NX>;
+  auto kern = k_grad_stream<TO, M, kStreamTY, kStreamS, NX>;
+  const int res = stream_resident(h, kern, L::total);
+  if (res == 0) return false;
+  const Geo g = geo(h);
+  const int yt = h->ny / kStreamTY, zc = stream_chunk(h->nz, yt, res);
+  kern<<<dim3(yt, (h->nz + zc - 1) / zc), 256, L::total, h->stream>>>(h->den, dx, dy, dz, h->st, g, zc,
+                                                                     &h->gred->err);
+  HE4_LAUNCHED(h);
+  return true;
+}
+
+#define HE4_NX_SWITCH(nx, ...)                 \
+  switch (nx) {                                \
+    case 64: {                                 \
+      constexpr int NX_ = 64;                  \
+      __VA_ARGS__;                             \
+    }                                          \
+    case 128: {                                \
+      constexpr int NX_ = 128;                 \
+      __VA_ARGS__;                             \
+    }                                          \
+    case 256: {                                \
+      constexpr int NX_ = 256;                 \
+      __VA_ARGS__;                             \
+    }                                          \
+    case 512: {                                \
+      constexpr int NX_ = 512;                 \
+      __VA_ARGS__;                             \
+    }                                          \
+    default: return false;                     \
+  }
+
+template <typename TO>
+static bool grad_stream(Handle *h, TO *dx, TO *dy, TO *dz) {
+  if (!stream_ok(h)) return false;
+  if (h->st.m == 3) {
+    HE4_NX_SWITCH(h->nx, return (launch_grad_stream<TO, 3, NX_>(h, dx, dy, dz)))
+  }
+  HE4_NX_SWITCH(h->nx, return (launch_grad_stream<TO, 6, NX_>(h, dx, dy, dz)))
+}
+
+template <typename TI, int M>
+static bool pot4_stream_m(Handle *h, const TI *lin, const TI *dcg, const TI *h0, const TI *h1, const TI *h2,
+                          const OtArgs &ot) {
+  if (h->p.core4 == HE4_CORE_OTC) {
+    HE4_NX_SWITCH(h->nx, return (launch_pot4_stream<TI, true, M, NX_>(h, lin, dcg, h0, h1, h2, ot)))
+  }
+  HE4_NX_SWITCH(h->nx, return (launch_pot4_stream<TI, false, M, NX_>(h, lin, dcg, h0, h1, h2, ot)))
+}
+
+template <typename TI>
+static bool pot4_stream(Handle *h, const TI *lin, const TI *dcg, const TI *h0, const TI *h1, const TI *h2,
+                        const OtArgs &ot) {
+  if (!stream_ok(h)) return false;
+  return h->st.m == 3 ? pot4_stream_m<TI, 3>(h, lin, dcg, h0, h1, h2, ot)
+                      : pot4_stream_m<TI, 6>(h, lin, dcg, h0, h1, h2, ot);
+}
+
 bool real32_ok(const Handle *h) { return h->fp32 && zmarch_ok(h); }
+
+// density gradient into the float grids g32[2..4] (FP32-convolution form)
+int launch_grad_f32(Handle *h) {
+  if (!h->real32) {
+    set_error("the float-grid gradient needs the FP32-convolution form's float grids");
+    return HE4_E_STATE;
+  }
+  const Geo g = geo(h);
+  float *gx = h->g32[2], *gy = h->g32[3], *gz = h->g32[4];
+  if (h->use_stream && grad_stream<float>(h, gx, gy, gz)) return HE4_OK;
+  if (h->st.m == 3)
+    k_grad_z_tile<3, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
+  else
+    k_grad_z_tile<6, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
+  HE4_LAUNCHED(h);
+  return HE4_OK;
+}
 
 int launch_grad(Handle *h) {
   const Geo g = geo(h);
@@ -610,11 +790,7 @@ static int field_poten_merged_f32(Handle *h) {
     float *out[2] = {dencg, denalf};
     HE4_TRY(fft_c2r_f32(h, otc ? 2 : 1, sp, out));
   }
-  if (h->st.m == 3)
-    k_grad_z_tile<3, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
-  else
-    k_grad_z_tile<6, kZB, float><<<grid_z(g), block3(), 0, h->stream>>>(h->den, gx, gy, gz, h->st, g);
-  HE4_LAUNCHED(h);
+  HE4_TRY(launch_grad_f32(h));
   {
     const void *in[1] = {h->den};
     double2 *sp[1] = {h->spec[5]};
@@ -677,6 +853,7 @@ int launch_pot4_merged_f32(Handle *h) {
   const bool otc = (h->p.core4 == HE4_CORE_OTC);
   const float *sl = h->g32[8], *dencg = h->g32[0];
   const float *h0 = otc ? h->g32[5] : nullptr, *h1 = otc ? h->g32[6] : nullptr, *h2 = otc ? h->g32[7] : nullptr;
+  if (h->use_stream && pot4_stream<float>(h, sl, dencg, h0, h1, h2, ot)) return HE4_OK;
   if (h->st.m == 3) {
     if (otc)
       k_pot4_merged_z<true, 3, kZBp, float, false><<<grid_z(g, kZBp), block3(), 0, h->stream>>>(sl, h->den, dencg, h0, h1,

@@ -594,29 +594,36 @@ def reference_arm(args):
     }), flush=True)
 
 
-def profile_kernels(form, config="c3"):
+def profile_kernels(form, config="c3", shape=None, ids=None, reps=1):
     """One field evaluation of a workload, then one warm-up and one timed
     launch of each pass he4_bench_kernel measures: the workload the ncu
-    summaries under profiles/ capture (the 128^3 config keeps a capture at
-    a few GB on the device)."""
+    summaries under profiles/ capture.  shape (nx, ny, nz) replaces the
+    grid of the config (the same spacing and droplet), so a capture keeps
+    its inputs above L2 with a few GB on the device."""
     pkg = load_pkg()
     w = pkg.workloads
-    p, psi, r, v, _ = w.workload(config)
+    if shape is None:
+        p, psi, r, v, _ = w.workload(config)
+    else:
+        cfg = w.CONFIGS[config]
+        p = w.make_params(shape[0], cfg["h"], cfg["npar"], ny=shape[1], nz=shape[2])
+        psi = w.droplet_psi(p, cfg["n4"])
+        r, v = w.particles(cfg["npar"], 1234, cfg["speed_ms"])
     g = pkg.He4Step(form_params(pkg, p, form))
     g.set_state(psi, r, v)
-    g.field()
+    g.run(1, w.deltat_fs(DT_FS))  # a merged evaluation fills the float grids
     L = pkg.load_library()
     L.he4_bench_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double), C.c_char_p, C.c_int32]
-    ids = (0, 1, 2, 3, 6, 7, 8) + ((9, 10) if form == "fp32" else ())
+    if ids is None:
+        ids = (0, 1, 2, 3, 6, 7, 8) + ((9, 10) if form == "fp32" else ())
     for which in ids:
-        g.field()
         ms, b = C.c_double(), C.c_double()
         nm = C.create_string_buffer(64)
-        if L.he4_bench_kernel(g._h, which, 1, C.byref(ms), C.byref(b), nm, 64) != 0:
+        if L.he4_bench_kernel(g._h, which, reps, C.byref(ms), C.byref(b), nm, 64) != 0:
             raise RuntimeError(L.he4_last_error().decode())
         print(json.dumps({"which": which, "kernel": nm.value.decode(), "algorithmic_bytes": b.value,
-                          "ms": ms.value}), flush=True)
+                          "ms": ms.value, "grid": [p.nx, p.ny, p.nz]}), flush=True)
     g.close()
 
 
@@ -637,9 +644,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-kernels", choices=["fp64", "fp32"], default=None,
                     help="run each FFT/stencil pass once on the --config workload (for ncu captures) and exit")
+    ap.add_argument("--profile-shape", default=None, help="nx,ny,nz grid for --profile-kernels")
+    ap.add_argument("--profile-reps", type=int, default=1, help="timed launches per id for --profile-kernels")
+    ap.add_argument("--profile-ids", default=None, help="comma-separated he4_bench_kernel ids for --profile-kernels")
     args = ap.parse_args()
     if args.profile_kernels:
-        profile_kernels(args.profile_kernels, args.config)
+        shape = tuple(int(x) for x in args.profile_shape.split(",")) if args.profile_shape else None
+        ids = tuple(int(x) for x in args.profile_ids.split(",")) if args.profile_ids else None
+        profile_kernels(args.profile_kernels, args.config, shape, ids, args.profile_reps)
         return
     if args.warmup < 3:
         args.warmup = 3
