@@ -21,6 +21,7 @@ HE4_POT_TABLE = 0
 HE4_POT_MORSE = 1
 HE4_POT_NULL = 2
 HE4_POT_RTABLE = 3
+HE4_POT_HE2S_FCI = 4
 
 HE4_PREC_FP64 = 0
 HE4_PREC_FP32CONV = 1

@@ -65,7 +65,7 @@ static int check_params(const he4_params *p) {
     return HE4_E_ARG;
   }
   if (p->pot_kind != HE4_POT_TABLE && p->pot_kind != HE4_POT_MORSE && p->pot_kind != HE4_POT_NULL &&
-      p->pot_kind != HE4_POT_RTABLE) {
+      p->pot_kind != HE4_POT_RTABLE && p->pot_kind != HE4_POT_HE2S_FCI) {
     set_error("unknown pot_kind %d", p->pot_kind);
     return HE4_E_ARG;
   }

@@ -285,13 +285,93 @@ static double rtable_eval(const RTable &t, double r) {
   return t.A[k] + r * (t.B[k] + r * (t.C[k] + r * t.D[k]));
 }
 
-// Select_Pot conventions (V_impur.f90:84-935): r < r_cutoff -> umax
+// Select_Pot conventions (V_impur.f90:84-935): r < r_cutoff -> umax.  The
+// caller-sampled table is evaluated here; the analytic entries run on the
+// device (k_pair_pot).
 static double pair_pot(const he4_params &p, const RTable *t, double r) {
   if (p.pot_kind == HE4_POT_NULL) return 0.0;
   if (r < p.r_cutoff) return p.umax;
-  if (p.pot_kind == HE4_POT_RTABLE) return rtable_eval(*t, r);
-  const double e = 1.0 - exp(-p.morse_alpha * (r - p.morse_re));
-  return p.morse_d * (e * e - 1.0);
+  return rtable_eval(*t, r);
+}
+
+// ---------------------------------------------------------------------------
+// analytic Select_Pot entries on the device
+// ---------------------------------------------------------------------------
+// double-double numbers (hi + lo, |lo| <= ulp(hi)/2): Knuth's two-sum and
+// the FMA two-product give the exact rounding errors of + and *; a
+// quotient takes one correction step on the residual
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+  const double s = a + b, bb = s - a;
+  return DD{s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ DD dd_fast_two_sum(double a, double b) {  // |a| >= |b|
+  const double s = a + b;
+  return DD{s, b - (s - a)};
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD s = dd_two_sum(a.hi, b.hi);
+  const DD t = dd_two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = dd_fast_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return dd_fast_two_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+  const double p = a.hi * b.hi;
+  const double e = fma(a.hi, b.hi, -p) + (a.hi * b.lo + a.lo * b.hi);
+  return dd_fast_two_sum(p, e);
+}
+__device__ __forceinline__ DD dd_recip(double x) {  // 1/x
+  const double q = 1.0 / x;
+  const double r = fma(-q, x, 1.0);  // exact residual 1 - q x
+  return dd_fast_two_sum(q, r / x);
+}
+
+// Pg(1..11) of Block Data Inicio_LJ_V_He2s_fci (V_impur.f90:2965-2980),
+// the real*16 decimal constants split into hi + lo doubles
+__constant__ double kHe2sPg[11][2] = {
+    {-0x1.42e15606a60a7p+26, 0x1.dd3a6436341a8p-28},  {0x1.47ef02a3e655bp+32, -0x1.eb16493dff276p-23},
+    {-0x1.27401c07c6057p+37, -0x1.a220013722c39p-18}, {0x1.35469e31e7656p+41, -0x1.358c7b5bdc35ep-14},
+    {-0x1.a0860d440150fp+44, -0x1.01b219d398bf1p-10}, {0x1.776e6d55a7e11p+47, 0x1.c4445ee71dc20p-7},
+    {-0x1.c92e2141b13a0p+49, 0x1.990ffee5e8bcap-5},   {0x1.72ca490c9d9abp+51, -0x1.7f2e612330a62p-3},
+    {-0x1.7f6ee42e976d9p+52, 0x1.9b19fd2a249b5p-11}, {0x1.c912072946918p+52, -0x1.491e80ea3b0f9p-2},
+    {-0x1.ddbc07afa638dp+51, -0x1.cf3f1e0d13c9ep-4}};
+
+// V_He2s_fci (V_impur.f90:2983-3008): fcutoff = 580.0065 K for
+// x <= 3.17502 A, else sum_k Pg(k) (1/x)^(5+k); the reference sums in
+// real*16, here in double-double, and rounds once to double
+__device__ double v_he2s_fci_dev(double x) {
+  if (x <= 3.17502) return 5.8000649999999996e+02;
+  const DD xq = dd_recip(x);
+  DD aux = dd_mul(xq, xq);        // xq^2
+  aux = dd_mul(aux, dd_mul(aux, aux));  // xq^6 = xq^(k0+1), k0 = 5
+  DD sto{0.0, 0.0};
+  for (int k = 0; k < 11; k++) {
+    sto = dd_add(sto, dd_mul(DD{kHe2sPg[k][0], kHe2sPg[k][1]}, aux));
+    aux = dd_mul(aux, xq);
+  }
+  return sto.hi + sto.lo;
+}
+
+struct PotArgs {
+  int kind;
+  double r_cutoff, umax, d, alpha, re;
+};
+
+__device__ double pair_pot_dev(const PotArgs &p, double r) {
+  if (p.kind == HE4_POT_NULL) return 0.0;
+  if (r < p.r_cutoff) return p.umax;
+  if (p.kind == HE4_POT_HE2S_FCI) return v_he2s_fci_dev(r);
+  const double e = 1.0 - exp(-p.alpha * (r - p.re));
+  return p.d * (e * e - 1.0);
+}
+
+__global__ void k_pair_pot(const double *__restrict__ r, int n, PotArgs p, double *__restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = pair_pot_dev(p, r[i]);
 }
 
 // cubic spline with end second derivatives s1, sn; global-form coefficients
@@ -430,23 +510,35 @@ static int build_vq(Handle *h, double qmax, double hq) {
     set_error("Vq table needs at least 4 q points (nq=%d)", P.nq);
     return HE4_E_ARG;
   }
-  RTable tab;
-  if (P.pot_kind == HE4_POT_RTABLE) HE4_TRY(rtable_build(P, &tab));
-  const RTable *t = &tab;
-  std::vector<double> x(N), y(N), A(N), B(N), C(N), D(N);
   const double X1 = P.r_cutoff + eps, XN = r_max;
-  const double S1 =
-      (pair_pot(P, t, X1) - 2.0 * pair_pot(P, t, X1 + dr) + pair_pot(P, t, X1 + dr + dr)) / (dr * dr);
-  const double Sn = (pair_pot(P, t, XN - dr) - 2.0 * pair_pot(P, t, XN) + pair_pot(P, t, XN + dr)) / (dr * dr);
   const double hr = (XN - X1) / (N - 1);
-  for (int i = 0; i < N; i++) {
-    x[i] = (double)i * hr + X1;
-    y[i] = pair_pot(P, t, x[i]);
-  }
-  HE4_TRY(spline_global(x.data(), y.data(), A.data(), B.data(), C.data(), D.data(), S1, Sn, N));
+  // V at the spline nodes, then at the six points of the end curvatures
+  std::vector<double> x(N + 6), y(N + 6), A(N), B(N), C(N), D(N);
+  for (int i = 0; i < N; i++) x[i] = (double)i * hr + X1;
+  const double ends[6] = {X1, X1 + dr, X1 + dr + dr, XN - dr, XN, XN + dr};
+  for (int i = 0; i < 6; i++) x[N + i] = ends[i];
   DevBuf<double> dx, dA, dB, dC, dD, dv;
   const size_t bytes = sizeof(double) * N;
-  HE4_CUDA_TRY(cudaMalloc(&dx.p, bytes));
+  HE4_CUDA_TRY(cudaMalloc(&dx.p, sizeof(double) * (N + 6)));
+  if (P.pot_kind == HE4_POT_RTABLE) {
+    RTable tab;
+    HE4_TRY(rtable_build(P, &tab));
+    for (int i = 0; i < N + 6; i++) y[i] = pair_pot(P, &tab, x[i]);
+  } else {
+    // Select_Pot on the device
+    DevBuf<double> dy;
+    HE4_CUDA_TRY(cudaMalloc(&dy.p, sizeof(double) * (N + 6)));
+    HE4_CUDA_TRY(cudaMemcpyAsync(dx.p, x.data(), sizeof(double) * (N + 6), cudaMemcpyHostToDevice, h->stream));
+    const PotArgs pa{P.pot_kind, P.r_cutoff, P.umax, P.morse_d, P.morse_alpha, P.morse_re};
+    k_pair_pot<<<(N + 6 + 255) / 256, 256, 0, h->stream>>>(dx.p, N + 6, pa, dy.p);
+    HE4_LAUNCHED(h);
+    HE4_CUDA_TRY(cudaMemcpyAsync(y.data(), dy.p, sizeof(double) * (N + 6), cudaMemcpyDeviceToHost, h->stream));
+    HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  const double *ye = y.data() + N;
+  const double S1 = (ye[0] - 2.0 * ye[1] + ye[2]) / (dr * dr);
+  const double Sn = (ye[3] - 2.0 * ye[4] + ye[5]) / (dr * dr);
+  HE4_TRY(spline_global(x.data(), y.data(), A.data(), B.data(), C.data(), D.data(), S1, Sn, N));
   HE4_CUDA_TRY(cudaMalloc(&dA.p, bytes));
   HE4_CUDA_TRY(cudaMalloc(&dB.p, bytes));
   HE4_CUDA_TRY(cudaMalloc(&dC.p, bytes));

@@ -186,6 +186,8 @@ void load_input(Run &r, const std::string &text) {
     p.morse_re = nl.real("morse_re", 5.5);
   } else if (selec == "null") {
     p.pot_kind = HE4_POT_NULL;
+  } else if (selec == "he2s_fci") {
+    p.pot_kind = HE4_POT_HE2S_FCI;  // evaluated by the library on the device
   } else {
     die("Select_Pot entry '" + selec +
         "' is not built into the library: sample its V(r) from r_cutoff_gs on into vrfile, or tabulate its Vq "

@@ -47,9 +47,14 @@ enum {
   HE4_POT_MORSE = 1, /* V(r)=D[(1-exp(-a(r-re)))^2-1], r<r_cutoff -> umax,  */
                      /* transformed by the FT_V_spline procedure           */
   HE4_POT_NULL = 2,  /* V = 0 ('null' entry of Select_Pot)                  */
-  HE4_POT_RTABLE = 3 /* caller samples V(r) (any Select_Pot entry) on a     */
-                     /* uniform r grid; splined, r<r_cutoff -> umax, 0 past */
-                     /* the last point, transformed by FT_V_spline          */
+  HE4_POT_RTABLE = 3, /* caller samples V(r) (any Select_Pot entry) on a    */
+                      /* uniform r grid; splined, r<r_cutoff -> umax, 0 past*/
+                      /* the last point, transformed by FT_V_spline         */
+  HE4_POT_HE2S_FCI = 4 /* Select_Pot 'He2S_fci' (V_impur.f90:179-183,       */
+                       /* 2962-3008): He(2S)-He, sum of Pg(k) r^-(5+k),     */
+                       /* k=1..11, evaluated on the device in double-double */
+                       /* arithmetic (the reference uses real*16), 580.0065 K*/
+                       /* inside 3.17502 A; r<r_cutoff -> umax as Select_Pot*/
 };
 
 /* Arithmetic of the convolution FFTs and the pointwise potential assembly.

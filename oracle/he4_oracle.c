@@ -550,11 +550,38 @@ static double rtab_eval(const rtab *t, double r) {
   return t->a[k] + r * (t->b[k] + r * (t->c[k] + r * t->d[k]));
 }
 
+/* V_He2s_fci (V_impur.f90:2962-3008), Eloranta's He(2S)-He potential:
+ * fcutoff for x <= rcutoff, |aa x^2 + bb x + cc| for x <= r0 (r0 = 0, never
+ * taken for x > 0), else sum_{k=1..11} Pg(k) (1/x)^(k0+k) with k0 = 5.  The
+ * reference keeps Pg, 1/x, the power and the sum in real*16; GCC's
+ * __float128 (IEEE binary128, the same format) restates that arithmetic. */
+static double v_he2s_fci(double x) {
+  static const __float128 pg[11] = {
+      -84641112.1038843174868366388591186Q,  5501813411.89974475880756271682097Q,
+      -158511366392.752661259845175521651Q,  2656659334094.79191838532512036583Q,
+      -28623286583317.0595767811072611642Q,  206395570574320.545052095736748454Q,
+      -1005349880685171.95006561484544998Q,  3261504889875669.31289981948240792Q,
+      -6745427649591000.99921588607933893Q,  8040867895208215.67859457559937689Q,
+      -4202197034021318.61309730280594230Q};
+  const double rcutoff = 3.17502, fcutoff = 5.8000649999999996e+02;
+  if (x <= rcutoff) return fcutoff;
+  __float128 xq = 1.0Q / (__float128)x, aux = 1.0Q, sto = 0.0Q;
+  for (int i = 0; i < 6; i++) aux = aux * xq; /* xq**(k0+1) */
+  for (int k = 0; k < 11; k++) {
+    sto = sto + pg[k] * aux;
+    aux = aux * xq;
+  }
+  return (double)sto;
+}
+
+double ora_v_he2s_fci(double x) { return v_he2s_fci(x); }
+
 /* Select_Pot conventions (V_impur.f90:84-935): r < r_cutoff -> umax. */
 static double pair_pot(const he4_params *p, const rtab *t, double r) {
   if (p->pot_kind == HE4_POT_NULL) return 0.0;
   if (r < p->r_cutoff) return p->umax;
   if (p->pot_kind == HE4_POT_RTABLE) return rtab_eval(t, r);
+  if (p->pot_kind == HE4_POT_HE2S_FCI) return v_he2s_fci(r);
   double e = 1.0 - exp(-p->morse_alpha * (r - p->morse_re));
   return p->morse_d * (e * e - 1.0);
 }

@@ -45,6 +45,7 @@ void ora_set_threads(int n);
 /* Building blocks exposed for pinning tests. */
 int ora_fd_weights(int npd, int id, double *w); /* centre row, no 1/h^id */
 double ora_si(double x);                        /* sine integral Si(x)   */
+double ora_v_he2s_fci(double x);                /* V_He2s_fci in K       */
 int ora_fft3_r2c(int nx, int ny, int nz, const double *in, double *out);
 int ora_fft3_c2r(int nx, int ny, int nz, const double *in, double *out);
 int ora_spline(const double *x, const double *y, double *a, double *b,

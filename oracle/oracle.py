@@ -60,6 +60,8 @@ def _declare(L):
     L.ora_fd_weights.argtypes = [C.c_int, C.c_int, dp]
     L.ora_si.argtypes = [C.c_double]
     L.ora_si.restype = C.c_double
+    L.ora_v_he2s_fci.argtypes = [C.c_double]
+    L.ora_v_he2s_fci.restype = C.c_double
     L.ora_fft3_r2c.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp]
     L.ora_fft3_c2r.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp]
     L.ora_spline.argtypes = [dp, dp, dp, dp, dp, dp, C.c_double, C.c_double, C.c_int]
@@ -91,6 +93,11 @@ def fd_weights(npd, order):
 
 def si(x):
     return lib().ora_si(float(x))
+
+
+def v_he2s_fci(x):
+    """V_He2s_fci(x) in K (binary128 sums, rounded to double)."""
+    return lib().ora_v_he2s_fci(float(x))
 
 
 def fft3_r2c(a):

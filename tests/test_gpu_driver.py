@@ -192,3 +192,53 @@ def test_driver_shipped_style_start(pkg, tmp_path):
     # the files hold 17 significant digits, so the start differs from the
     # driver's in the last place
     assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+
+
+def test_driver_shipped_namelist_without_host_potential(pkg, ora, tmp_path):
+    """The shipped namelist's potential entry (Selec_gs='He2S_fci',
+    r_cutoff_gs, umax_gs; data_files/input_He2S.0:2) runs with no vrfile or
+    vqfile: the library evaluates Select_Pot on the device.  A 32x32x40 grid,
+    mode 0 start, icon=13, npd=13, ironx=3 and the absorbing layer as in the
+    shipped inputs; the driver's final state equals the oracle's run from
+    the start the driver wrote, and its Vq the oracle's to one FP32 ulp."""
+    w = pkg.workloads
+    d = str(tmp_path)
+    nx, nz, h = 32, 40, 0.6
+    p = w.make_params(nx, h, 200, npd=13, nz=nz, pot=pkg.abi.HE4_POT_HE2S_FCI, nq=1500)
+    p.icon = 13
+    p.ironx = 3
+    p.r_cutoff, p.umax = 3.17502, 580.0065
+    p.lambdah, p.tzmean, p.tzsurf = 2.0, 10.0, 1.0
+    x, y, z = w.grid_axes(p)
+    den = np.abs(w.droplet_psi(p, 150)) ** 2
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    denx = np.exp(-((X - 0.3) ** 2 + Y ** 2 + (Z - 1.0) ** 2) / 0.5)
+    for name, f in (("den.inp", den), ("denx.inp", denx)):
+        with open(os.path.join(d, name), "w") as fh:
+            fh.write(f"# start\n {p.xmax!r} {p.ymax!r} {p.zmax!r} {h!r} {h!r} {h!r} {p.nx} {p.ny} {p.nz} T 0. 0. 0.\n")
+            fh.write("\n".join(f" {v:.17E}" for v in f.reshape(-1)) + "\n")
+    nml = f""" &input
+ Selec_gs='He2S_fci', r_cutoff_gs=3.17502d0, umax_gs=5.800065d2
+ nx={p.nx}, ny={p.ny}, nz={p.nz}, xmax={p.xmax!r}, ymax={p.ymax!r}, zmax={p.zmax!r},
+ n4=150, mode=0, filedenin='den.inp', fileimpin='denx.inp', core4='OTC', npd=13, icon=13,
+ N_par={p.n_par}, mimpur=4.002602d0, ironx=3, Lambdah=2.d0, tzmean=10.d0, tzsurf=1.d0,
+ xi=-1.5d0, xf=2.d0, yi=-1.5d0, yf=1.5d0, zi=-0.5d0, zf=2.5d0, v0z=-1.d0, seed=5,
+ deltatps=1.d-3, niter=5, pener=5, pcurr=0, Nq=1500 /
+"""
+    res = subprocess.run([os.path.join(PKG, "he4run")], input=nml, capture_output=True, text=True, cwd=d)
+    assert res.returncode == 0, res.stderr[-2000:]
+    psi0 = read_psi(os.path.join(d, "density.000.dat"), den.shape)
+    _, r0, v0 = read_particles(os.path.join(d, "densityx.000.dat"))
+    got = read_psi(os.path.join(d, "he4.output.density"), den.shape)
+    o = ora.Oracle(p)
+    with pkg.He4Step(p) as g:
+        gv, ov = g.get_kernel("vq"), o.get_kernel("vq")
+        ulp = np.spacing(np.abs(ov).astype(np.float32)).astype(np.float64)
+        assert np.all(np.abs(gv - ov) <= ulp)
+    o.set_state(psi0, r0, v0)
+    o.run(5, w.deltat_fs(1.0))
+    want = o.get_state()[0]
+    o.close()
+    # the oracle builds its own Vq (1-ulp FP32 flips possible) and the start
+    # files hold 17 significant digits
+    assert np.max(np.abs(got - want)) <= 1e-9 * np.max(np.abs(want))

@@ -83,6 +83,26 @@ def test_vq_from_sampled_potential(pkg, ora):
         pkg.He4Step(q)
 
 
+def test_vq_of_the_he2s_fci_entry(pkg, ora):
+    """HE4_POT_HE2S_FCI: Select_Pot's 'He2S_fci' potential evaluated on the
+    device (double-double sums) and transformed by FT_V_spline, against the
+    oracle (binary128 sums) to one FP32 ulp, with the shipped inputs'
+    r_cutoff_gs and umax_gs (data_files/input_He2S.0:2)."""
+    p = pkg.workloads.make_params(48, 0.5, 8, pot=pkg.abi.HE4_POT_HE2S_FCI, nq=1500)
+    p.r_cutoff, p.umax = 3.17502, 580.0065
+    o = ora.Oracle(p)
+    want = o.get_kernel("vq")
+    o.close()
+    with pkg.He4Step(p) as g:
+        got = g.get_kernel("vq")
+    ulp = np.spacing(np.abs(want).astype(np.float32)).astype(np.float64)
+    assert np.all(np.abs(got - want) <= ulp)
+    assert np.mean(got == want) > 0.99
+    # not the Morse kernel by accident
+    with pkg.He4Step(pkg.workloads.make_params(48, 0.5, 8, nq=1500)) as g:
+        assert np.max(np.abs(g.get_kernel("vq") - got)) > 1e-3 * np.max(np.abs(got))
+
+
 @pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 80), (48, 40, 30)])
 def test_fft_against_numpy_and_cufft(pkg, shape):
     import ctypes as C

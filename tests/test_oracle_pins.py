@@ -276,3 +276,51 @@ def test_field_consistency_free_droplet(pkg, ora):
     assert e["eHeX"] == 0.0 and e["ekinqx"] == 0.0
     assert e["etot4"] < 0  # a bound droplet
     o.close()
+
+
+def test_he2s_fci_oracle_matches_exact_sums(ora):
+    """The oracle's V_He2s_fci (binary128 sums like the reference's real*16)
+    against the exact rational sums of the reference's decimal constants
+    (tests/golden/he2s_fci.json, made by make_he2s.py): within one double
+    ulp, and fcutoff at and inside the 3.17502 A cutoff."""
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "he2s_fci.json")))
+    for r, v in zip(d["r"], d["v"]):
+        want = float.fromhex(v)
+        got = ora.v_he2s_fci(r)
+        assert abs(got - want) <= np.spacing(abs(want)), (r, got, want)
+    assert ora.v_he2s_fci(3.0) == d["fcutoff"]
+
+
+def test_vq_of_he2s_fci_matches_quadrature(pkg, ora):
+    """Vq of the 'He2S_fci' entry (FT_V_spline of V_He2s_fci, r < r_cutoff
+    -> umax) from the oracle against scipy quadrature of the same capped
+    potential (4 pi / q int r V(r) sin(q r) dr, q = 2 pi |p|)."""
+    w = pkg.workloads
+    p = w.make_params(32, 0.5, 8, pot=pkg.abi.HE4_POT_HE2S_FCI, nq=400)
+    p.r_cutoff, p.umax = 3.17502, 580.0065
+    o = ora.Oracle(p)
+    vq = o.get_kernel("vq")
+    pm = o.get_kernel("pmod")
+    o.close()
+    rc, um = p.r_cutoff, p.umax
+
+    def V(r):
+        return um if r < rc else ora.v_he2s_fci(r)
+
+    def ft(pv):
+        if pv == 0:
+            outer, _ = scipy.integrate.quad(lambda r: r * r * V(r), rc, 200, limit=400)
+            return 4 * math.pi * (um * rc ** 3 / 3 + outer)
+        q = 2 * math.pi * pv
+        inner, _ = scipy.integrate.quad(lambda r: r * um, 0, rc, weight="sin", wvar=q)
+        outer, _ = scipy.integrate.quad(lambda r: r * V(r), rc, 200, weight="sin", wvar=q, limit=2000)
+        return 4 * math.pi / q * (inner + outer)
+
+    scale = abs(vq[0, 0, 0])
+    for idx in [(1, 0, 0), (3, 2, 1), (6, 5, 4), (8, 8, 8)]:
+        assert vq[idx] == pytest.approx(ft(pm[idx]), rel=2e-5, abs=2e-5 * scale), idx
+    # q = 0 comes from the small-q refit (FT_V_spline.f90:230-264), a spline
+    # through the transform at four larger q extrapolated to 0, not from the
+    # integral itself: measured 1.9e-4 below the quadrature for this
+    # potential's steep core
+    assert vq[0, 0, 0] == pytest.approx(ft(0.0), rel=5e-4)
