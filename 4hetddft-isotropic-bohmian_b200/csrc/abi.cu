@@ -48,8 +48,12 @@ static int check_params(const he4_params *p) {
     set_error("npd=%d exceeds a grid dimension", p->npd);
     return HE4_E_ARG;
   }
-  if (p->icon != 8 && p->icon != 13) {
-    set_error("icon=%d: only periodic (icon=8) and zero-padded (icon=13) boundaries are implemented", p->icon);
+  if (p->icon != 8 && p->icon != 12 && p->icon != 13) {
+    set_error("icon=%d: periodic (icon=8) and Redef's icon=12 and icon=13 boundaries are implemented", p->icon);
+    return HE4_E_UNSUPPORTED;
+  }
+  if (p->icon == 12 && p->npd > 15) {
+    set_error("icon=12 needs npd <= 15 (one-sided boundary rows of the Bickley matrix)");
     return HE4_E_UNSUPPORTED;
   }
   if (p->core4 != HE4_CORE_OT && p->core4 != HE4_CORE_OTC) {
@@ -104,7 +108,7 @@ static void free_all(Handle *h) {
                   h->dyden, h->dzden, h->penalty, h->corr, h->denx, h->psix, h->hpsix, h->uimp, h->fx, h->fy,
                   h->fz, h->rtmp[0], h->rtmp[1], h->rtmp[2], h->rtmp[3], h->counts, h->rimp, h->vimp, h->aimp,
                   h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0], h->vimpold[1], h->vimpold[2],
-                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->bub, h->box, h->gred,
+                  h->aimpold[0], h->aimpold[1], h->qr, h->qv, h->pcr, h->pcv, h->red, h->scal, h->bub, h->box, h->gred, h->st_lo,
                   h->k32[0], h->k32[1], h->k32[2], h->k32[3], h->dsym32};
   for (void *p : ptrs) cudaFree(p);
   for (int i = 0; i < 9; i++) cudaFree(h->g32[i]);

@@ -98,8 +98,12 @@ struct Stencil {
   int m = 3;                 // half width, npd = 2m+1
   double w1[3][25];          // first derivative, per axis
   double w2[3][25];          // second derivative, per axis
+  // icon=12: device table [order-1][axis][c < m][2m+1] of the one-sided
+  // Bickley rows of the first m points, times 1/h^order (null otherwise)
+  const double *lo = nullptr;
 };
 int fd_weights(int npd, int order, double *w);
+int fd_rows(int npd, int order, double *rows);
 
 struct ZOp;  // z-pass operation (fft.cu)
 
@@ -206,6 +210,7 @@ struct Handle {
 
   // reductions
   GridRed *gred = nullptr;    // particle-kernel partials, counters, box scratch
+  double *st_lo = nullptr;    // icon=12 boundary rows (Stencil::lo)
   double *red = nullptr;      // partial sums workspace
   double *scal = nullptr;     // device scalars (errors, energies, means)
   double *hscal = nullptr;    // pinned host mirror of scal

@@ -32,9 +32,9 @@ __global__ void k_energy(const double2 *__restrict__ psi, const double *__restri
   double v[kESums] = {0, 0, 0, 0, 0, 0, 0};
   if (i < g.nx && j < g.ny) {
     const size_t t = ((size_t)k * g.ny + j) * g.nx + i;
-    const double2 d1 = stencil_axis_c(psi, st.w1[0], st.m, g, i, j, k, 0);
-    const double2 d2 = stencil_axis_c(psi, st.w1[1], st.m, g, i, j, k, 1);
-    const double2 d3 = stencil_axis_c(psi, st.w1[2], st.m, g, i, j, k, 2);
+    const double2 d1 = stencil_axis_c(psi, st, 1, g, i, j, k, 0);
+    const double2 d2 = stencil_axis_c(psi, st, 1, g, i, j, k, 1);
+    const double2 d3 = stencil_axis_c(psi, st, 1, g, i, j, k, 2);
     v[0] = (d1.x * d1.x + d1.y * d1.y) + (d2.x * d2.x + d2.y * d2.y) + (d3.x * d3.x + d3.y * d3.y);
     const double dn = den[t], dc = dencg[t];
     v[1] = delj4[t] * dn;
@@ -61,7 +61,7 @@ __global__ void k_sumsq(const double *__restrict__ x, int n, double *out) {
 }
 
 int compute_energy(Handle *h, he4_energies *E) {
-  const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
+  const Geo g{h->nx, h->ny, h->nz, zpad_of(h->p.icon)};
   const he4_params &p = h->p;
   EArgs a;
   a.aux1 = 0.5 * p.cp4;

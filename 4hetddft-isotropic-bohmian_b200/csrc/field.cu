@@ -15,14 +15,14 @@
 
 namespace he4 {
 
-static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0}; }
+static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz, zpad_of(h->p.icon)}; }
 
 // derden (derden.f90:26-28)
 __global__ void k_grad(const double *__restrict__ f, double *dx, double *dy, double *dz, Stencil st, Geo g) {
   HE4_IJK(g);
-  dx[t] = stencil_axis(f, st.w1[0], st.m, g, i, j, k, 0);
-  dy[t] = stencil_axis(f, st.w1[1], st.m, g, i, j, k, 1);
-  dz[t] = stencil_axis(f, st.w1[2], st.m, g, i, j, k, 2);
+  dx[t] = stencil_axis(f, st, 1, g, i, j, k, 0);
+  dy[t] = stencil_axis(f, st, 1, g, i, j, k, 1);
+  dz[t] = stencil_axis(f, st, 1, g, i, j, k, 2);
 }
 
 // The same stencils for a compile-time half width M, one CTA of 32 x 8
@@ -341,9 +341,9 @@ __global__ void k_alfa2m(const T *dx, const T *dy, const T *dz, const T *ix, con
 __global__ void k_alfa3(double *ualphas, const double *__restrict__ h0, const double *__restrict__ h1,
                         const double *__restrict__ h2, double *pot4, Stencil st, Geo g, OtArgs a) {
   HE4_IJK(g);
-  const double d0 = stencil_axis(h0, st.w1[0], st.m, g, i, j, k, 0);
-  const double d1 = stencil_axis(h1, st.w1[1], st.m, g, i, j, k, 1);
-  const double d2 = stencil_axis(h2, st.w1[2], st.m, g, i, j, k, 2);
+  const double d0 = stencil_axis(h0, st, 1, g, i, j, k, 0);
+  const double d1 = stencil_axis(h1, st, 1, g, i, j, k, 1);
+  const double d2 = stencil_axis(h2, st, 1, g, i, j, k, 2);
   const double u = ualphas[t] / a.den0s;
   const double ua = (u + d0 + d1 + d2) * a.h2o2m4 * a.alphas;
   ualphas[t] = ua;
@@ -375,9 +375,9 @@ __global__ void k_pot4_merged(const double *__restrict__ lin, const double *__re
   const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0;
   double v = lin[t] + dc * dc * (a0 + a1 * dc) + pen;
   if (OTC) {
-    const double d0 = stencil_axis(h0, st.w1[0], st.m, g, i, j, k, 0);
-    const double d1 = stencil_axis(h1, st.w1[1], st.m, g, i, j, k, 1);
-    const double d2 = stencil_axis(h2, st.w1[2], st.m, g, i, j, k, 2);
+    const double d0 = stencil_axis(h0, st, 1, g, i, j, k, 0);
+    const double d1 = stencil_axis(h1, st, 1, g, i, j, k, 1);
+    const double d2 = stencil_axis(h2, st, 1, g, i, j, k, 2);
     v += (d0 + d1 + d2) * a.h2o2m4 * a.alphas;
   }
   pot4[t] = v;

@@ -211,9 +211,9 @@ __global__ void k_lap_box(const BoxPair *__restrict__ bp, const double *__restri
                           double scale, Stencil st, Geo g) {
   const Box b = bp->cur;
   HE4_BOX_LOOP(b, st.m, g)
-  const double a = stencil_axis(psix, st.w2[0], st.m, g, i, j, k, 0);
-  const double bb = stencil_axis(psix, st.w2[1], st.m, g, i, j, k, 1);
-  const double c = stencil_axis(psix, st.w2[2], st.m, g, i, j, k, 2);
+  const double a = stencil_axis(psix, st, 2, g, i, j, k, 0);
+  const double bb = stencil_axis(psix, st, 2, g, i, j, k, 1);
+  const double c = stencil_axis(psix, st, 2, g, i, j, k, 2);
   hpsix[t] = scale * ((a + bb) + c);
   HE4_BOX_END
 }
@@ -232,8 +232,8 @@ __global__ void k_force_q_box(const BoxPair *__restrict__ bp, double *fx, double
     double *F[3] = {fx, fy, fz};
 #pragma unroll
     for (int ax = 0; ax < 3; ax++) {
-      const double dps = stencil_axis(psix, st.w1[ax], st.m, g, i, j, k, ax);
-      const double dhp = stencil_axis(hpsix, st.w1[ax], st.m, g, i, j, k, ax);
+      const double dps = stencil_axis(psix, st, 1, g, i, j, k, ax);
+      const double dhp = stencil_axis(hpsix, st, 1, g, i, j, k, ax);
       F[ax][t] = F[ax][t] + inv * (dps * hp - ps * dhp) / mass;
     }
   }
@@ -263,7 +263,7 @@ static unsigned box_grid(const Handle *h) {
 }
 
 int impurity_density(Handle *h) {
-  const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
+  const Geo g{h->nx, h->ny, h->nz, zpad_of(h->p.icon)};
   const DepArgs d = dep_args(h);
   const unsigned gb = box_grid(h);
   const unsigned pg = (unsigned)std::max(1, std::min(kPartMaxCta, (h->npar + kPartThreads - 1) / kPartThreads));
@@ -290,7 +290,7 @@ int impurity_density(Handle *h) {
 }
 
 int impurity_force_q(Handle *h) {
-  const Geo g{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0};
+  const Geo g{h->nx, h->ny, h->nz, zpad_of(h->p.icon)};
   k_force_q_box<<<box_grid(h), 256, 0, h->stream>>>(h->box, h->fx, h->fy, h->fz, h->psix, h->hpsix, h->denx,
                                                    h->mAg_u, h->st, g);
   HE4_LAUNCHED(h);

@@ -107,6 +107,49 @@ int fd_weights(int npd, int order, double *w) {
   return HE4_OK;
 }
 
+// The whole npd x npd Bickley matrix of order `order` (newder.f:99-125 with
+// ICON=1; BLOCK DATA BLKDS, mates.f:172-14043): rows[c * npd + j] is the
+// order-th derivative at node c of the Lagrange basis polynomial of node j
+// over the nodes 0..npd-1 (unit spacing).  Exact integers (the basis
+// numerator's coefficients, its denominator prod (j - q)), rounded once to
+// nearest; the table's entries are these rationals.  npd <= 15 keeps every
+// intermediate inside 128 bits.
+int fd_rows(int npd, int order, double *rows) {
+  typedef __int128 i128;
+  if (npd < 3 || npd > 15 || npd % 2 == 0 || (order != 1 && order != 2)) return HE4_E_ARG;
+  for (int j = 0; j < npd; j++) {
+    i128 coef[16] = {0};  // prod_{q != j} (x - q), ascending powers
+    coef[0] = 1;
+    int deg = 0;
+    i128 den = 1;
+    for (int q = 0; q < npd; q++) {
+      if (q == j) continue;
+      for (int d = deg + 1; d >= 1; d--) coef[d] = coef[d - 1] - (i128)q * coef[d];
+      coef[0] = -(i128)q * coef[0];
+      deg++;
+      den *= (i128)(j - q);
+    }
+    for (int c = 0; c < npd; c++) {
+      i128 v = 0;
+      for (int d = order; d <= deg; d++) {
+        i128 f = 1, pw = 1;
+        for (int u = 0; u < order; u++) f *= (i128)(d - u);
+        for (int u = 0; u < d - order; u++) pw *= (i128)c;
+        v += coef[d] * f * pw;
+      }
+      const bool neg = (v < 0) != (den < 0);
+      const u128 num = (u128)(v < 0 ? -v : v), dd = (u128)(den < 0 ? -den : den);
+      double r = 0.0;
+      if (num != 0) {
+        const u128 g = gcd_u128(num, dd);
+        r = div_round_nearest(num / g, dd / g);
+      }
+      rows[c * npd + j] = neg ? -r : r;
+    }
+  }
+  return HE4_OK;
+}
+
 // ---------------------------------------------------------------------------
 // device special functions
 // ---------------------------------------------------------------------------
@@ -663,6 +706,25 @@ int setup_kernels(Handle *h) {
     HE4_TRY(fd_weights(P.npd, 2, w));
     sto = 1.0 / (hh[ax] * hh[ax]);
     for (int j = 0; j < 25; j++) h->st.w2[ax][j] = (j < P.npd) ? w[j] * sto : 0.0;
+  }
+  // icon=12: the one-sided rows of the first m points (rows 1..ko2 that
+  // Redef leaves untouched, redef.f:133-150), scaled as the centre rows
+  if (P.icon == 12) {
+    const int m = h->st.m, K = P.npd;
+    std::vector<double> r1((size_t)K * K), r2((size_t)K * K), lo((size_t)2 * 3 * m * K);
+    HE4_TRY(fd_rows(K, 1, r1.data()));
+    HE4_TRY(fd_rows(K, 2, r2.data()));
+    for (int ax = 0; ax < 3; ax++) {
+      const double s1 = 1.0 / hh[ax], s2 = 1.0 / (hh[ax] * hh[ax]);
+      for (int c = 0; c < m; c++)
+        for (int t = 0; t < K; t++) {
+          lo[((size_t)(0 * 3 + ax) * m + c) * K + t] = r1[(size_t)c * K + t] * s1;
+          lo[((size_t)(1 * 3 + ax) * m + c) * K + t] = r2[(size_t)c * K + t] * s2;
+        }
+    }
+    HE4_CUDA_TRY(cudaMalloc((void **)&h->st_lo, sizeof(double) * lo.size()));
+    HE4_CUDA_TRY(cudaMemcpy(h->st_lo, lo.data(), sizeof(double) * lo.size(), cudaMemcpyHostToDevice));
+    h->st.lo = h->st_lo;
   }
   // imaginary part of the first-derivative symbol per axis:
   // D(k) = i * 2 sum_{t=1..m} w_t sin(2 pi t k / n)

@@ -21,7 +21,7 @@
 
 namespace he4 {
 
-static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz, h->p.icon == 13 ? 1 : 0}; }
+static Geo geo(const Handle *h) { return Geo{h->nx, h->ny, h->nz, zpad_of(h->p.icon)}; }
 
 __global__ void k_finalize_sums(const double *__restrict__ part, size_t stride, int nb, int nvals, double mult,
                                 double div, double *out) {

@@ -72,7 +72,9 @@ typedef struct he4_params {
   int32_t nx, ny, nz;
   double xmax, ymax, zmax;
   /* derivatives (module deriva): npd odd in [3,25]; icon 8 = periodic,
-   * icon 13 = centred stencils with f = 0 outside the grid (redef.f:133-170) */
+   * icon 13 = centred stencils with f = 0 outside the grid (redef.f:133-170),
+   * icon 12 = the same at the upper end and the Bickley matrix's one-sided
+   * rows for the first npd/2 points (redef.f:133-150; npd <= 15) */
   int32_t npd, icon;
   /* functional */
   int32_t core4;

@@ -109,6 +109,65 @@ static u128 fact128(int n) {
   return f;
 }
 
+/* Exact rationals in 128 bits for the boundary rows below. */
+typedef struct { __int128 n, d; } rat;
+static __int128 iabs128(__int128 a) { return a < 0 ? -a : a; }
+static rat rat_make(__int128 n, __int128 d) {
+  if (d < 0) { n = -n; d = -d; }
+  u128 g = gcd128((u128)iabs128(n), (u128)d);
+  if (g > 1) { n /= (__int128)g; d /= (__int128)g; }
+  rat r = {n, d};
+  return r;
+}
+static rat rat_sub(rat a, rat b) { return rat_make(a.n * b.d - b.n * a.d, a.d * b.d); }
+static rat rat_mul(rat a, rat b) {
+  rat x = rat_make(a.n, b.d), y = rat_make(b.n, a.d); /* cross-reduce first */
+  return rat_make(x.n * y.n, x.d * y.d);
+}
+static rat rat_div(rat a, rat b) { rat inv = rat_make(b.d, b.n); return rat_mul(a, inv); }
+static rat rat_int(long v) { rat r = {(__int128)v, 1}; return r; }
+
+/* The whole npd x npd Bickley matrix for derivative order id (newder.f:99-125
+ * with ICON=1, table BLKDS in mates.f): row c holds the weights of the
+ * derivative at node c over the nodes 0..npd-1 (unit spacing).  Fornberg's
+ * recursion (Math. Comp. 51, 699 (1988)) for the weights of every derivative
+ * up to id, in exact rational arithmetic, each weight rounded once to
+ * nearest.  npd <= 15. */
+int ora_fd_rows(int npd, int id, double *rows) {
+  if (npd < 3 || npd > 15 || (npd % 2) == 0 || (id != 1 && id != 2)) return HE4_E_ARG;
+  for (int c = 0; c < npd; c++) {
+    rat C[15][3];
+    for (int j = 0; j < npd; j++)
+      for (int k = 0; k <= 2; k++) C[j][k] = rat_int(0);
+    rat c1 = rat_int(1), c4 = rat_int(0 - c);
+    C[0][0] = rat_int(1);
+    for (int i = 1; i < npd; i++) {
+      int mn = i < 2 ? i : 2;
+      rat c2 = rat_int(1), c5 = c4;
+      c4 = rat_int(i - c);
+      for (int j = 0; j < i; j++) {
+        rat c3 = rat_int(i - j);
+        c2 = rat_mul(c2, c3);
+        if (j == i - 1) {
+          for (int k = mn; k >= 1; k--)
+            C[i][k] = rat_div(rat_mul(c1, rat_sub(rat_mul(rat_int(k), C[i - 1][k - 1]), rat_mul(c5, C[i - 1][k]))), c2);
+          C[i][0] = rat_div(rat_mul(rat_mul(rat_int(-1), c1), rat_mul(c5, C[i - 1][0])), c2);
+        }
+        for (int k = mn; k >= 1; k--)
+          C[j][k] = rat_div(rat_sub(rat_mul(c4, C[j][k]), rat_mul(rat_int(k), C[j][k - 1])), c3);
+        C[j][0] = rat_div(rat_mul(c4, C[j][0]), c3);
+      }
+      c1 = c2;
+    }
+    for (int j = 0; j < npd; j++) {
+      rat w = C[j][id];
+      double v = (w.n == 0) ? 0.0 : ratio_rn((u128)iabs128(w.n), (u128)w.d);
+      rows[c * npd + j] = (w.n < 0) ? -v : v;
+    }
+  }
+  return HE4_OK;
+}
+
 /* Centre row of the npd-point Bickley derivative matrix for derivative order
  * id (1 or 2), i.e. Cdc(id, ko2p1, :) of Init_deriv_p
  * (init_deriv_parallel.f90:72-78, newder.f:99-125 with ICON=1), without the
@@ -713,6 +772,7 @@ struct ora_state {
   double *x, *y, *z, *timec_re; /* timec_re [nz] */
   double *pmod, *wcgk, *fvlj4, *kalfs, *vq; /* [H] */
   double w1[3][25], w2[3][25]; /* stencil weights including 1/h^id */
+  double lo1[3][7][15], lo2[3][7][15]; /* icon=12: rows 1..ko2 of the matrix, times 1/h^id */
   fft3 F;
   /* He */
   cplx *psi, *psiold[3], *hpsiold[2], *q, *pc;
@@ -823,7 +883,8 @@ int ora_create(const he4_params *pin, ora_state **out) {
   if (!pin || !out) return HE4_E_ARG;
   const he4_params *p = pin;
   if (!valid_n(p->nx) || !valid_n(p->ny) || !valid_n(p->nz)) return HE4_E_ARG;
-  if (p->icon != 8 && p->icon != 13) return HE4_E_UNSUPPORTED;
+  if (p->icon != 8 && p->icon != 12 && p->icon != 13) return HE4_E_UNSUPPORTED;
+  if (p->icon == 12 && p->npd > 15) return HE4_E_UNSUPPORTED;
   if (p->npd < 3 || p->npd > 25 || p->npd % 2 == 0) return HE4_E_ARG;
   if (p->n_par < 1 || p->ironx < 0) return HE4_E_ARG;
   if (p->core4 != HE4_CORE_OT && p->core4 != HE4_CORE_OTC) return HE4_E_UNSUPPORTED;
@@ -932,6 +993,20 @@ int ora_create(const he4_params *pin, ora_state **out) {
       sto = 1.0 / (h[ax] * h[ax]);
       for (int j = 0; j < p->npd; j++) s->w2[ax][j] = w[j] * sto;
     }
+    /* icon=12: Redef (redef.f:133-150) rewrites only the rows after the
+     * centre, so the first ko2 points keep the matrix's own rows */
+    if (p->icon == 12) {
+      double r1[15 * 15], r2[15 * 15];
+      int K = p->npd, m = K / 2;
+      ora_fd_rows(K, 1, r1);
+      ora_fd_rows(K, 2, r2);
+      for (int ax = 0; ax < 3; ax++)
+        for (int c = 0; c < m; c++)
+          for (int t = 0; t < K; t++) {
+            s->lo1[ax][c][t] = r1[c * K + t] * (1.0 / h[ax]);
+            s->lo2[ax][c][t] = r2[c * K + t] * (1.0 / (h[ax] * h[ax]));
+          }
+    }
   }
   if (fft3_init(&s->F, nx, ny, nz)) { ora_destroy(s); return HE4_E_UNSUPPORTED; }
   /* arrays (dimen.f90) */
@@ -986,19 +1061,30 @@ void ora_destroy(ora_state *s) {
 /* (init_deriv_parallel.f90:373-655 and 938-1213).  icon=8: periodic.       */
 /* icon=13: Redef (redef.f:133-170) replaces the ko2 boundary rows at each   */
 /* end by the centre row shifted one place per row, its taps past the end   */
-/* dropped, i.e. the centred stencil with f = 0 outside the grid.            */
+/* dropped, i.e. the centred stencil with f = 0 outside the grid.  icon=12: */
+/* the same at the upper end only; the first ko2 points keep the matrix's   */
+/* one-sided rows (init_deriv_parallel.f90:429-435).                         */
 /* ------------------------------------------------------------------------ */
 
 static void deriv_r(const ora_state *s, int id, int axis, const double *f, double *df) {
   int nx = s->nx, ny = s->ny, nz = s->nz, m = s->p.npd / 2;
   const double *w = (id == 1) ? s->w1[axis] : s->w2[axis];
-  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz, zpad = (s->p.icon == 13);
+  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz, zpad = (s->p.icon != 8), one_sided = (s->p.icon == 12);
+  size_t st = (axis == 0) ? 1 : (axis == 1) ? (size_t)nx : (size_t)nx * ny;
   if (n < s->p.npd) { memset(df, 0, sizeof(double) * s->N); return; }
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++) {
         double acc = 0.0;
+        int cc = (axis == 0) ? i : (axis == 1) ? j : k;
+        if (one_sided && cc < m) { /* df(i) = sum_j Cd(i, j) f(j), j = 1..npd */
+          const double *L = (id == 1) ? s->lo1[axis][cc] : s->lo2[axis][cc];
+          size_t base = ((size_t)k * ny + j) * nx + i - (size_t)cc * st;
+          for (int t = 0; t < s->p.npd; t++) acc += L[t] * f[base + (size_t)t * st];
+          df[((size_t)k * ny + j) * nx + i] = acc;
+          continue;
+        }
         for (int t = -m; t <= m; t++) {
           int ii = i, jj = j, kk = k;
           if (zpad) {
@@ -1017,13 +1103,26 @@ static void deriv_r(const ora_state *s, int id, int axis, const double *f, doubl
 static void deriv_c(const ora_state *s, int id, int axis, const cplx *f, cplx *df) {
   int nx = s->nx, ny = s->ny, nz = s->nz, m = s->p.npd / 2;
   const double *w = (id == 1) ? s->w1[axis] : s->w2[axis];
-  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz, zpad = (s->p.icon == 13);
+  int n = (axis == 0) ? nx : (axis == 1) ? ny : nz, zpad = (s->p.icon != 8), one_sided = (s->p.icon == 12);
+  size_t st = (axis == 0) ? 1 : (axis == 1) ? (size_t)nx : (size_t)nx * ny;
   if (n < s->p.npd) { memset(df, 0, sizeof(cplx) * s->N); return; }
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++) {
         double ar = 0.0, ai = 0.0;
+        int cc = (axis == 0) ? i : (axis == 1) ? j : k;
+        if (one_sided && cc < m) {
+          const double *L = (id == 1) ? s->lo1[axis][cc] : s->lo2[axis][cc];
+          size_t base = ((size_t)k * ny + j) * nx + i - (size_t)cc * st;
+          for (int t = 0; t < s->p.npd; t++) {
+            cplx v = f[base + (size_t)t * st];
+            ar += L[t] * creal(v);
+            ai += L[t] * cimag(v);
+          }
+          df[((size_t)k * ny + j) * nx + i] = ar + I * ai;
+          continue;
+        }
         for (int t = -m; t <= m; t++) {
           int ii = i, jj = j, kk = k;
           if (zpad) {

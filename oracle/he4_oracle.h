@@ -44,6 +44,7 @@ void ora_set_threads(int n);
 
 /* Building blocks exposed for pinning tests. */
 int ora_fd_weights(int npd, int id, double *w); /* centre row, no 1/h^id */
+int ora_fd_rows(int npd, int id, double *rows); /* whole matrix, npd<=15 */
 double ora_si(double x);                        /* sine integral Si(x)   */
 double ora_v_he2s_fci(double x);                /* V_He2s_fci in K       */
 int ora_fft3_r2c(int nx, int ny, int nz, const double *in, double *out);

@@ -58,6 +58,7 @@ def _declare(L):
     L.ora_set_threads.argtypes = [C.c_int]
     L.ora_set_threads.restype = None
     L.ora_fd_weights.argtypes = [C.c_int, C.c_int, dp]
+    L.ora_fd_rows.argtypes = [C.c_int, C.c_int, dp]
     L.ora_si.argtypes = [C.c_double]
     L.ora_si.restype = C.c_double
     L.ora_v_he2s_fci.argtypes = [C.c_double]
@@ -89,6 +90,13 @@ def fd_weights(npd, order):
     w = np.zeros(npd)
     _check(lib().ora_fd_weights(npd, order, _dp(w)), "ora_fd_weights")
     return w
+
+
+def fd_rows(npd, order):
+    """The whole npd x npd Bickley matrix (rows = nodes), no 1/h^order."""
+    w = np.zeros(npd * npd)
+    _check(lib().ora_fd_rows(npd, order, _dp(w)), "ora_fd_rows")
+    return w.reshape(npd, npd)
 
 
 def si(x):

@@ -10,8 +10,11 @@ derivatives (icon=8) use only the centre row Cdc(K, (M+1)/2, :)
 (init_deriv_parallel.f90:72-78, 475-650).
 
 This script parses the DATA statements as text, rebuilds the centre rows for
-K = 1, 2 and writes them as exact hex floats to blkds_central.json.  It is run
-once, in a checkout that has the reference sources; the JSON is committed.
+K = 1, 2 and writes them as exact hex floats to blkds_central.json, and the
+whole matrices for M = 3..15, K = 1, 2 to blkds_full.json (the icon=12
+boundary uses rows 1..M/2 of them, init_deriv_parallel.f90:429-435).  It is
+run once, in a checkout that has the reference sources; the JSON is
+committed.
 
 Usage: python make_blkds.py /path/to/reference/mates.f
 """
@@ -104,7 +107,13 @@ def main():
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "blkds_central.json"), "w") as f:
         json.dump({"source": "mates.f BLOCK DATA BLKDS (centre rows, K=1,2)", "rows": out}, f, indent=1)
-    print(f"wrote {len(out)} rows")
+    full = {}
+    for M in range(3, 16, 2):
+        for K in (1, 2):
+            full[f"{M}_{K}"] = [float(v).hex() for v in matrix(A, M, K)]
+    with open(os.path.join(here, "blkds_full.json"), "w") as f:
+        json.dump({"source": "mates.f BLOCK DATA BLKDS (whole matrices, row-major, K=1,2)", "matrices": full}, f)
+    print(f"wrote {len(out)} rows and {len(full)} matrices")
 
 
 if __name__ == "__main__":

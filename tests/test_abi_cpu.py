@@ -89,10 +89,13 @@ def test_errors_are_codes_not_aborts(pkg, lib):
     rc = lib.he4_create(C.byref(p), C.byref(h))
     assert rc == abi.HE4_E_ARG and not h.value
     assert b"grid" in lib.he4_last_error()
-    # boundary modes other than icon 8 (periodic) and 13 (zero-padded) are
-    # not implemented
+    # boundary modes other than icon 8 (periodic), 12 and 13 (Redef's rows)
+    # are not implemented, nor icon 12 past npd 15
     p = pkg.params_default()
-    p.icon = 12
+    p.icon = 4
+    assert lib.he4_create(C.byref(p), C.byref(h)) == abi.HE4_E_UNSUPPORTED
+    p = pkg.params_default()
+    p.icon, p.npd = 12, 17
     assert lib.he4_create(C.byref(p), C.byref(h)) == abi.HE4_E_UNSUPPORTED
     # null handle everywhere
     assert lib.he4_field(None) == abi.HE4_E_ARG
@@ -114,6 +117,10 @@ def test_create_without_device_fails_cleanly(pkg, lib):
 
 def test_oracle_rejects_what_the_library_rejects(pkg, ora):
     p = pkg.abi.default_params()
-    p.icon = 12
+    p.icon = 4
+    with pytest.raises(ora.OracleError):
+        ora.Oracle(p)
+    p = pkg.abi.default_params()
+    p.icon, p.npd = 12, 17
     with pytest.raises(ora.OracleError):
         ora.Oracle(p)

@@ -190,6 +190,48 @@ def test_field_and_steps_parity_icon13(pkg, c1_icon13):
             assert abs(Eg[k] - Eo[k]) <= 1e-10 * max(abs(Eo[k]), 1e-30), (k, Eg[k], Eo[k])
 
 
+def test_field_and_steps_parity_icon12(pkg, ora):
+    """icon=12 (redef.f:133-150): zero-padded centred rows at the upper end,
+    the Bickley matrix's one-sided rows for the first ko2 points; npd 7 and
+    13 on a droplet that reaches the box faces.  Fields after one evaluation
+    within 1e-11 of the oracle, 3 RK + 5 PC steps within 1e-10, and the
+    lower-end rows are live (icon=13 gives another density gradient)."""
+    w = pkg.workloads
+    for npd in (7, 13):
+        p = w.make_params(48, 0.6, 256, npd=npd, nz=40)
+        p.icon = 12
+        psi = w.droplet_psi(p, 350)
+        r, v = w.particles(256, 77, 100.0)
+        o = ora.Oracle(p)
+        vq = o.get_kernel("vq")
+        o.set_state(psi, r, v)
+        o.field()
+        with gpu_with_table(pkg, p, vq) as g:
+            g.set_state(psi, r, v)
+            g.field()
+            for name in pkg.abi.FIELDS:
+                assert rel(g.get_field(name), o.get_field(name)) < 1e-11, (npd, name)
+            q = pkg.abi.He4Params.from_buffer_copy(p)
+            q.icon = 13
+            with gpu_with_table(pkg, q, vq) as g13:
+                g13.set_state(psi, r, v)
+                g13.field()
+                assert rel(g13.get_field("dxden"), g.get_field("dxden")) > 1e-6
+        dt = w.deltat_fs(1.0)
+        o.set_state(psi, r, v)
+        eo, mo = o.run(8, dt)
+        with gpu_with_table(pkg, p, vq) as g:
+            g.set_state(psi, r, v)
+            eg, mg = g.run(8, dt)
+            assert np.allclose(eg[3:], eo[3:], rtol=1e-8, atol=0)
+            assert np.allclose(mg, mo, rtol=1e-9, atol=1e-9 * np.abs(mo).max())
+            assert rel(g.get_state()[0], o.get_state()[0]) < 1e-10
+            Eg, Eo = g.energy(), o.energy()
+            for k in Eo:
+                assert abs(Eg[k] - Eo[k]) <= 1e-10 * max(abs(Eo[k]), 1e-30), (npd, k, Eg[k], Eo[k])
+        o.close()
+
+
 def test_steps_parity(pkg, c1):
     p, psi, r, v, o, vq = c1
     dt = pkg.workloads.deltat_fs(1.0)

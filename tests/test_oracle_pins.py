@@ -237,6 +237,65 @@ def redef13_rows(c, n):
     return D
 
 
+def test_fd_rows_match_reference_matrices_bitwise(ora):
+    """The oracle's whole Bickley matrices (exact rationals by Fornberg's
+    recursion, rounded once) equal the reference's table (mates.f BLKDS,
+    tests/golden/blkds_full.json) bit for bit, npd 3..15, orders 1 and 2."""
+    mats = json.load(open(os.path.join(HERE, "golden", "blkds_full.json")))["matrices"]
+    assert len(mats) == 14
+    for key, hexes in mats.items():
+        npd, order = map(int, key.split("_"))
+        want = np.array([float.fromhex(h) for h in hexes]).reshape(npd, npd)
+        assert np.array_equal(ora.fd_rows(npd, order), want), key
+
+
+def redef12_rows(rows, c, n):
+    """Deriv3D_p's matrix for icon=12 built as Redef does it
+    (redef.f:133-150): only the ko2 rows after the centre row are rewritten
+    (the centre row shifted right one place per row, the vacated entry
+    zero); the ko2 rows before it stay the matrix's own one-sided rows.
+    Row i < ko2 acts on f(1..k), row i > n-1-ko2 on f(n-k+1..n), the rest
+    is the centre row around i."""
+    k = len(c)
+    ko2 = k // 2
+    cd = np.array(rows, dtype=float)
+    cd[ko2] = c
+    for i in range(ko2 + 1, k):
+        cd[i, 1:] = cd[i - 1, :k - 1]
+        cd[i, 0] = 0.0
+    D = np.zeros((n, n))
+    for i in range(n):
+        if i < ko2:
+            D[i, :k] = cd[i]
+        elif i >= n - ko2:
+            D[i, n - k:] = cd[i - n + k]
+        else:
+            D[i, i - ko2:i + ko2 + 1] = c
+    return D
+
+
+@pytest.mark.parametrize("npd", [7, 13])
+def test_icon12_stencils_are_redef_rows(pkg, ora, npd):
+    """icon=12: the oracle's derivatives equal the matrix Redef builds from
+    the reference's own table rows, along each axis, for both orders."""
+    mats = json.load(open(os.path.join(HERE, "golden", "blkds_full.json")))["matrices"]
+    p = pkg.workloads.make_params(16, 0.6, 8, npd=npd, ny=20, nz=24)
+    p.icon = 12
+    o = ora.Oracle(p)
+    rng = np.random.default_rng(4)
+    f = rng.standard_normal((p.nz, p.ny, p.nx))
+    h = 2 * p.xmax / p.nx
+    for order in (1, 2):
+        full = np.array([float.fromhex(x) for x in mats[f"{npd}_{order}"]]).reshape(npd, npd)
+        c = full[npd // 2]
+        for axis, n in ((0, p.nx), (1, p.ny), (2, p.nz)):
+            D = redef12_rows(full, c, n) * (1.0 / h ** order)
+            want = np.moveaxis(np.tensordot(D, np.moveaxis(f, 2 - axis, 0), axes=(1, 0)), 0, 2 - axis)
+            got = o.deriv(f, order, axis)
+            assert np.allclose(got, want, rtol=1e-13, atol=1e-12 * np.max(np.abs(want))), (order, axis)
+    o.close()
+
+
 @pytest.mark.parametrize("npd", [7, 13])
 def test_icon13_stencils_are_redef_rows(pkg, ora, npd):
     """icon=13 (the shipped inputs' boundary mode): the oracle's derivatives
