@@ -873,6 +873,13 @@ int he4_get_stream(he4_handle *hh, void **stream) {
 
 int64_t he4_launch_count(he4_handle *hh) { return hh ? hh->h.launches : -1; }
 
+int he4_graph_stats(he4_handle *hh, int64_t *captured, int64_t *uncaptured) {
+  HANDLE_OR_FAIL(hh);
+  if (captured) *captured = h->graph_captures;
+  if (uncaptured) *uncaptured = h->steps_uncaptured;
+  return HE4_OK;
+}
+
 const char *he4_strerror(int code) {
   switch (code) {
     case HE4_OK: return "ok";

@@ -144,7 +144,7 @@ static std::vector<StepState> batch_state(he4_batch *b, double dt) {
 static bool same_state(const std::vector<StepState> &a, const std::vector<StepState> &b) {
   if (a.size() != b.size()) return false;
   for (size_t i = 0; i < a.size(); i++)
-    if (memcmp(&a[i], &b[i], sizeof(StepState)) != 0) return false;
+    if (!same_step_state(a[i], b[i])) return false;
   return true;
 }
 

@@ -141,6 +141,21 @@ struct StepState {
   int ioldp[3], ioldh[2], ioldr[3], ioldv[3], iolda[2];
   double dt;
 };
+// member by member (a byte comparison would also compare the padding after
+// iolda, which struct copies need not preserve: a state would then miss its
+// captured graph and be captured again, or run uncaptured)
+inline bool same_step_state(const StepState &a, const StepState &b) {
+  if (a.psi != b.psi || a.ctmp != b.ctmp || a.dt != b.dt) return false;
+  for (int i = 0; i < 3; i++)
+    if (a.psiold[i] != b.psiold[i] || a.rimpold[i] != b.rimpold[i] || a.vimpold[i] != b.vimpold[i] ||
+        a.ioldp[i] != b.ioldp[i] || a.ioldr[i] != b.ioldr[i] || a.ioldv[i] != b.ioldv[i])
+      return false;
+  for (int i = 0; i < 2; i++)
+    if (a.hpsiold[i] != b.hpsiold[i] || a.aimpold[i] != b.aimpold[i] || a.ioldh[i] != b.ioldh[i] ||
+        a.iolda[i] != b.iolda[i])
+      return false;
+  return true;
+}
 
 struct StepGraph {
   StepState before, after;
@@ -239,6 +254,7 @@ struct Handle {
   // captured PC steps (one per distinct StepState; the states repeat)
   std::vector<StepGraph> graphs;
   int use_graphs = 1;
+  int64_t graph_captures = 0, steps_uncaptured = 0;  // he4_graph_stats
   // row-streamed (bulk-copy pipelined) stencils where the grid allows them
   int use_stream = 1;
 };

@@ -505,13 +505,14 @@ int run_pc_graphs(Handle *h, int n, double dt, double *dres) {
     const StepState now = get_step_state(h, dt);
     StepGraph *hit = nullptr;
     for (StepGraph &g : h->graphs)
-      if (memcmp(&g.before, &now, sizeof(StepState)) == 0) {
+      if (same_step_state(g.before, now)) {
         hit = &g;
         break;
       }
     if (!hit && h->graphs.size() < kMaxGraphs) {
       StepGraph g;
       HE4_TRY(capture_pc(h, dt, &g));
+      h->graph_captures++;
       set_step_state(h, g.before);
       h->graphs.push_back(g);
       hit = &h->graphs.back();
@@ -525,6 +526,7 @@ int run_pc_graphs(Handle *h, int n, double dt, double *dres) {
       HE4_CUDA_TRY(cudaMemcpyAsync(dres + 12 * (size_t)s, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToDevice,
                                    h->stream));
     } else {
+      h->steps_uncaptured++;
       HE4_TRY(step_pc(h, dt, dres + 12 * (size_t)s));
     }
   }

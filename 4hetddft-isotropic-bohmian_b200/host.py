@@ -71,6 +71,7 @@ def load_library():
     L.he4_batch_launch_count.restype = C.c_int64
     L.he4_launch_count.argtypes = [vp]
     L.he4_launch_count.restype = C.c_int64
+    L.he4_graph_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.he4_strerror.argtypes = [C.c_int]
     L.he4_strerror.restype = C.c_char_p
     L.he4_last_error.argtypes = []
@@ -254,6 +255,12 @@ class He4Step:
 
     def launch_count(self):
         return int(load_library().he4_launch_count(self._h))
+
+    def graph_stats(self):
+        """(graphs captured, PC steps run uncaptured) of he4_run."""
+        cap, unc = C.c_int64(), C.c_int64()
+        _check(load_library().he4_graph_stats(self._h, C.byref(cap), C.byref(unc)), "he4_graph_stats")
+        return cap.value, unc.value
 
 
 class He4Batch:

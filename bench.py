@@ -207,9 +207,10 @@ def gpu_arm(args):
         sf = torch.cuda.ExternalStream(gf.stream(), device=torch.device("cuda", local))
         ms_f, launches_f, clocks_f = timed_run(gf, sf)
         ms_step = ms_f / args.steps
+        cap, unc = gf.graph_stats()
         forms[form] = {"form": FORMS[form], "ms_per_step": ms_step,
                        "value": replica_throughput(world, sim_ps, ms_f * 1e-3), "gpu_launches": launches_f,
-                       "clocks": clocks_f}
+                       "clocks": clocks_f, "graphs": {"captured": cap, "steps_uncaptured": unc}}
         # whole-step roofline: the algorithmic bytes of one PC step over its time
         peak, _ = load_peaks()
         sb = step_bytes(form, p.nx * p.ny * p.nz)
@@ -346,6 +347,7 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
         e2e_s = time.perf_counter() - t0
     clocks = clk.summary()
     launches = sum(h.launch_count() for h in par.handles) - n_lib0 + net.launches
+    gstats = [h.graph_stats() for h in par.handles]
     par.close()
     # accuracy against the plain FP64 sequential run over the same time
     with pkg.He4Step(p) as g64:
@@ -368,6 +370,7 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
             "vs_plain_fp64_serial": {"density_rel_l2": float(np.linalg.norm(dpar - d64) / np.linalg.norm(d64)),
                                      "etot_rel_diff": abs(epar["etot"] - e64["etot"]) / abs(e64["etot"])},
             "gpu_launches": launches, "clocks": clocks,
+            "graphs": {"captured": sum(c for c, _ in gstats), "steps_uncaptured": sum(u for _, u in gstats)},
             "e2e_h2d": psi.nbytes + r.nbytes + v.nbytes,
             "e2e_d2h": psi.nbytes + r.nbytes + v.nbytes}
 

@@ -267,6 +267,11 @@ int he4_device_ptr(he4_handle *h, int32_t which, void **ptr);
 /* Number of kernels this handle has launched (graph launches count the
  * kernels inside the graph). */
 int64_t he4_launch_count(he4_handle *h);
+/* CUDA-graph use of he4_run: how many PC-step graphs the handle captured
+ * (one per distinct buffer rotation of the step, at most 24) and how many
+ * PC steps ran uncaptured (launched one kernel at a time) because no
+ * captured graph matched.  Has no counterpart in the reference. */
+int he4_graph_stats(he4_handle *h, int64_t *captured, int64_t *uncaptured);
 
 /* Tile shapes of the FFT passes: tiles = {n1 x, n1 y, n1 z, px, wy, wz}.
  * For axis lengths 16..256 (powers of two) n1 is the four-step split

@@ -233,8 +233,12 @@ def test_driver_shipped_namelist_without_host_potential(pkg, ora, tmp_path):
     o = ora.Oracle(p)
     with pkg.He4Step(p) as g:
         gv, ov = g.get_kernel("vq"), o.get_kernel("vq")
+        # one FP32 ulp, or the FP64 rounding of the radial integrals (summed
+        # in another order on the device, ~1e-14 of the scale) where Vq is
+        # near zero and its FP32 ulp is smaller than that
         ulp = np.spacing(np.abs(ov).astype(np.float32)).astype(np.float64)
-        assert np.all(np.abs(gv - ov) <= ulp)
+        assert np.all(np.abs(gv - ov) <= ulp + 1e-13 * np.max(np.abs(ov)))
+        assert np.mean(gv == ov) > 0.99
     o.set_state(psi0, r0, v0)
     o.run(5, w.deltat_fs(1.0))
     want = o.get_state()[0]
