@@ -206,6 +206,13 @@ static int create(const he4_params *pin, Handle *h) {
                         &h->vimpold[0], &h->vimpold[1], &h->vimpold[2], &h->aimpold[0], &h->aimpold[1],
                         &h->qr, &h->qv, &h->pcr, &h->pcv};
   for (double **f : pfields) HE4_TRY(dalloc(f, P3));
+  {
+    double2 *hc[7] = {h->psi, h->ctmp, h->psiold[0], h->psiold[1], h->psiold[2], h->hpsiold[0], h->hpsiold[1]};
+    double *hp[8] = {h->rimpold[0], h->rimpold[1], h->rimpold[2], h->vimpold[0],
+                     h->vimpold[1], h->vimpold[2], h->aimpold[0], h->aimpold[1]};
+    memcpy(h->home_c, hc, sizeof(hc));
+    memcpy(h->home_p, hp, sizeof(hp));
+  }
   // per-CTA partial sums of the grid reductions (7 energy sums max)
   const size_t nblocks = (size_t)((p.nx + 31) / 32) * ((p.ny + 7) / 8) * p.nz;
   h->red_len = 8 * nblocks;
@@ -332,6 +339,20 @@ int he4_set_state(he4_handle *hh, const double *psi, const double *rimp, const d
     return HE4_E_ARG;
   }
   const size_t N = h->N, P3 = 3 * (size_t)h->npar;
+  // the rotating buffers back in their allocation order: the steps from
+  // here walk the same cycle of buffer states as every earlier run, so the
+  // graphs captured then are replayed (the contents are all rewritten below)
+  h->psi = h->home_c[0];
+  h->ctmp = h->home_c[1];
+  for (int i = 0; i < 3; i++) {
+    h->psiold[i] = h->home_c[2 + i];
+    h->rimpold[i] = h->home_p[i];
+    h->vimpold[i] = h->home_p[3 + i];
+  }
+  for (int i = 0; i < 2; i++) {
+    h->hpsiold[i] = h->home_c[5 + i];
+    h->aimpold[i] = h->home_p[6 + i];
+  }
   HE4_CUDA_TRY(cudaMemcpyAsync(h->psi, psi, sizeof(double2) * N, cudaMemcpyDefault, h->stream));
   HE4_CUDA_TRY(cudaMemcpyAsync(h->rimp, rimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));
   HE4_CUDA_TRY(cudaMemcpyAsync(h->vimp, vimp, sizeof(double) * P3, cudaMemcpyDefault, h->stream));

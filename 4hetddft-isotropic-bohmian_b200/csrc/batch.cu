@@ -8,8 +8,12 @@
 // graph forks from a master stream into every member's stream, holds that
 // member's whole predictor-corrector step, and joins back, so the members'
 // kernels overlap on the GPU: small grids that leave most SMs idle on their
-// own fill the machine together.  The ring indices of the PC histories
-// repeat with period 6, so at most six graphs are captured and then replayed.
+// own fill the machine together.  A graph holds K consecutive ensemble
+// steps (K = 30, 10, 5 or 1, the largest the remaining steps allow), so a
+// run of 30 steps is one graph launch: each member's branch chains its K
+// steps, and the branches run side by side.  The members' buffer states
+// repeat with period 30 (the ψ buffers' rotation), so the graphs of one
+// cycle are captured once and replayed.
 #include <string.h>
 
 #include <algorithm>
@@ -109,6 +113,7 @@ using namespace he4;
 // ---------------------------------------------------------------------------
 struct EnsembleGraph {
   std::vector<StepState> before, after;
+  int ksteps = 1;  // ensemble steps per launch
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t kernels = 0;
@@ -149,8 +154,9 @@ static bool same_state(const std::vector<StepState> &a, const std::vector<StepSt
 }
 
 // one ensemble PC step captured from the current member states
-static int batch_capture(he4_batch *b, double dt, EnsembleGraph *out) {
+static int batch_capture(he4_batch *b, double dt, int ksteps, EnsembleGraph *out) {
   EnsembleGraph g;
+  g.ksteps = ksteps;
   g.before = batch_state(b, dt);
   std::vector<int64_t> l0, d0;
   for (he4_handle *hh : b->m) {
@@ -164,11 +170,14 @@ static int batch_capture(he4_batch *b, double dt, EnsembleGraph *out) {
     Handle *h = &b->m[i]->h;
     ce = cudaStreamWaitEvent(h->stream, b->fork, 0);
     if (ce != cudaSuccess) break;
-    rc = step_pc(h, dt, h->scal);
+    for (int s = 0; s < ksteps && rc == HE4_OK && ce == cudaSuccess; s++) {
+      rc = step_pc(h, dt, h->scal);
+      if (rc != HE4_OK) break;
+      k_batch_acc<<<1, 32, 0, h->stream>>>(h->scal, b->acc + 16 * i);
+      h->launches++;
+      ce = cudaGetLastError();
+    }
     if (rc != HE4_OK) break;
-    k_batch_acc<<<1, 32, 0, h->stream>>>(h->scal, b->acc + 16 * i);
-    h->launches++;
-    ce = cudaGetLastError();
     if (ce == cudaSuccess) ce = cudaEventRecord(b->capjoin[i], h->stream);
     if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->master, b->capjoin[i], 0);
   }
@@ -402,24 +411,27 @@ int he4_batch_run(he4_batch *b, int32_t nsteps, double deltat, double *err_max, 
         HE4_TRY(stream_after(b->master, h->stream, b->join[i]));
       }
     const std::vector<StepState> now = batch_state(b, deltat);
+    const int left = nsteps - s;
+    const int ks = left >= 30 ? 30 : left >= 10 ? 10 : left >= 5 ? 5 : 1;
     EnsembleGraph *hit = nullptr;
     for (EnsembleGraph &g : b->graphs)
-      if (same_state(g.before, now)) {
+      if (g.ksteps == ks && same_state(g.before, now)) {
         hit = &g;
         break;
       }
     if (!hit) {
-      if (b->graphs.size() >= 12) batch_free_graphs(b);
+      if (b->graphs.size() >= 64) batch_free_graphs(b);
       EnsembleGraph g;
-      HE4_TRY(batch_capture(b, deltat, &g));
+      HE4_TRY(batch_capture(b, deltat, ks, &g));
       b->graphs.push_back(g);
       hit = &b->graphs.back();
     }
     HE4_CUDA_TRY(cudaGraphLaunch(hit->exec, b->master));
+    s += hit->ksteps - 1;  // the loop adds the last one
     for (int i = 0; i < n; i++) {
       Handle *h = &b->m[i]->h;
       set_step_state(h, hit->after[i]);
-      h->nsteps_done++;
+      h->nsteps_done += hit->ksteps;
       h->field_valid = 1;
       h->split_valid = 0;
       h->forces_full = 0;

@@ -222,6 +222,11 @@ struct Handle {
   double *rimpold[3] = {nullptr}, *vimpold[3] = {nullptr}, *aimpold[2] = {nullptr};
   double *qr = nullptr, *qv = nullptr, *pcr = nullptr, *pcv = nullptr;
   int ioldp[3] = {0, 1, 2}, ioldh[2] = {0, 1}, ioldr[3] = {0, 1, 2}, ioldv[3] = {0, 1, 2}, iolda[2] = {0, 1};
+  // the buffers as allocated: he4_set_state puts every rotating pointer
+  // back here, so each run from a new state walks the same 30 step states
+  // (and reuses their captured graphs)
+  double2 *home_c[7] = {nullptr};   // psi, ctmp, psiold[0..2], hpsiold[0..1]
+  double *home_p[8] = {nullptr};    // rimpold[0..2], vimpold[0..2], aimpold[0..1]
 
   // reductions
   GridRed *gred = nullptr;    // particle-kernel partials, counters, box scratch

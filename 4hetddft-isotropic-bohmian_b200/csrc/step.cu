@@ -463,7 +463,12 @@ void free_graphs(Handle *h) {
   h->graphs.clear();
 }
 
-constexpr size_t kMaxGraphs = 24;
+// The PC step's buffer states repeat with period 30: the two swaps per step
+// (psi with the history slot ioldp(3), then psi with ctmp) permute the five
+// psi buffers with order 5, and the ring indices have period 6.  One graph
+// per state; he4_set_state restores the allocation order, so every run
+// walks the same 30 states.
+constexpr size_t kMaxGraphs = 30;
 
 // Capture one PC step from the current state (results into h->scal).  The
 // host state advances exactly as an eager step would; the graph has not run.

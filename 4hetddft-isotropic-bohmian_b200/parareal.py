@@ -220,6 +220,22 @@ class Parareal:
             h.close()
         self.handles = []
 
+    def warm(self, psi0, r0, v0):
+        """Captures the step graphs of every fine-propagator handle (the
+        starter plus one PC step of each of the 30 buffer states) from the
+        given state; he4_set_state puts the buffers back in allocation
+        order, so the runs that follow replay these graphs.  Like an FFT
+        plan, this is set-up work done once per handle."""
+        torch = self.torch
+        psi = torch.from_numpy(np.ascontiguousarray(psi0).view(np.float64).reshape(self.U[0].psi.shape)).to(self.dev)
+        r = torch.from_numpy(np.ascontiguousarray(r0)).to(self.dev)
+        v = torch.from_numpy(np.ascontiguousarray(v0)).to(self.dev)
+        torch.cuda.synchronize(self.dev)
+        for h in self.handles:
+            h.set_state_device(psi.data_ptr(), r.data_ptr(), v.data_ptr())
+            h.run(3 + 30, self.dt)
+        torch.cuda.synchronize(self.dev)
+
     def _fine(self, slices):
         """F(U_n) -> F[n+1] for the given slices, concurrently."""
         torch = self.torch

@@ -286,8 +286,11 @@ int he4_get_tiles(he4_handle *h, int32_t tiles[6]);
 int he4_tune(he4_handle *h, int32_t reps, double *best_ms, int32_t tiles[6]);
 
 /* Batched ensemble: n independent systems (grids may differ; one device)
- * advanced together, one CUDA graph launch per ensemble PC step (every
- * member's step is a parallel branch of the graph).  Members are ordinary
+ * advanced together by CUDA graphs that each hold K consecutive ensemble
+ * PC steps (K = 30, 10, 5 or 1, the largest the remaining steps allow;
+ * every member's K steps are one parallel branch of the graph), so 30
+ * steps are one graph launch.  The graphs are captured on first use and
+ * replayed; the members' buffer states repeat every 30 steps.  Members are ordinary
  * handles: he4_set_state / he4_get_state / he4_energy on
  * he4_batch_member(b, i) work as for any handle and are ordered after the
  * ensemble's work.  he4_batch_tune tunes one member per distinct grid and

@@ -36,6 +36,7 @@ def test_ensemble_matches_individual_runs(pkg):
         e, means = b.run(11, dt)
         assert b.launch_count() > n0
         e2, _ = b.run(4, dt)  # graphs replayed across calls
+        e3, _ = b.run(37, dt)  # a 30-step graph, then 5, 1 and 1
         got = [mem.get_state() for mem in b.members]
         energies = [mem.energy()["etot"] for mem in b.members]
     for (p, psi, r, v), (gpsi, gr, gv, _), et in zip(ms, got, energies):
@@ -43,6 +44,7 @@ def test_ensemble_matches_individual_runs(pkg):
             g.set_state(psi, r, v)
             g.run(11, dt)
             g.run(4, dt)
+            g.run(37, dt)
             spsi, sr, sv, _ = g.get_state()
             assert np.array_equal(gpsi, spsi)
             assert np.array_equal(gr, sr) and np.array_equal(gv, sv)

@@ -315,6 +315,23 @@ def test_run_equals_single_steps_and_is_deterministic(pkg, c1):
         assert np.array_equal(np.array(es), e1[3:])
 
 
+def test_step_graphs_cover_the_cycle_and_survive_set_state(pkg, c1):
+    """The PC step's buffer states repeat every 30 steps: he4_run captures
+    30 graphs and runs no step uncaptured, and a new he4_set_state (which
+    puts the buffers back in allocation order) replays them."""
+    p, psi, r, v, o, vq = c1
+    dt = pkg.workloads.deltat_fs(1.0)
+    with gpu_with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        g.run(3 + 45, dt)
+        assert g.graph_stats() == (30, 0)
+        a = g.get_state()[0]
+        g.set_state(psi, r, v)
+        g.run(3 + 45, dt)
+        assert g.graph_stats() == (30, 0)
+        assert np.array_equal(g.get_state()[0], a)
+
+
 @pytest.mark.parametrize("variant", ["npd13", "ot_core", "noncubic", "edge"])
 def test_field_parity_variants(pkg, ora, variant):
     """Other stencil widths, the 'OT ' core, a non-cubic grid, and particles
