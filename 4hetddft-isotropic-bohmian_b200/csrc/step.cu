@@ -527,7 +527,12 @@ int run_pc_graphs(Handle *h, int n, double dt, double *dres) {
       h->launches += hit->kernels;
       set_step_state(h, hit->after);
       h->nsteps_done++;
+      // what the captured step's merged evaluation leaves, as step_pc does:
+      // pot4 and the forces of the new state, not the split fields (delj4,
+      // uimp, ...) nor the forces outside the particle box
       h->field_valid = 1;
+      h->split_valid = 0;
+      h->forces_full = 0;
       HE4_CUDA_TRY(cudaMemcpyAsync(dres + 12 * (size_t)s, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToDevice,
                                    h->stream));
     } else {
