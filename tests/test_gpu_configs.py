@@ -16,6 +16,10 @@
     integrator handles between steps 203 and 503 at dt = 1 fs in both
     forms (he4_run returns HE4_E_NONFINITE), so the 2000-step length of its
     definition cannot be compared; 203 steps is the compared window.
+  * 128^3: 3 RK + 300 PC steps (the last stable stretch) against the
+    oracle, then 20 more steps, in which the GPU run stops with
+    HE4_E_NONFINITE and the oracle's state goes non-finite too: the
+    breakdown is the method's on this input, not a device artefact.
   * ensemble members of the 96^3 and 128^3 grids (1024 particles each),
     advanced together in one He4Batch with autotuned tiles, 3 RK + 5 PC.
 Tolerances: psi and pot4 1e-10 of their largest values, each energy term
@@ -135,6 +139,27 @@ def test_medium_droplet_fp32_form_per_term(pkg):
         assert abs(E32[k] - E64[k]) <= tol * max(abs(E64[k]), 1e-30), (k, E32[k], E64[k])
     assert np.linalg.norm(d32 - d64) / np.linalg.norm(d64) < 1e-6
     assert abs(n32 - n64) < 1e-8 * n64
+
+
+def test_medium_droplet_stable_window_and_breakdown(pkg, ora):
+    w = pkg.workloads
+    p, psi, r, v, _ = w.workload("c2")
+    dt = w.deltat_fs(1.0)
+    o = ora.Oracle(p)
+    vq = o.get_kernel("vq")
+    with with_table(pkg, p, vq) as g:
+        g.set_state(psi, r, v)
+        o.set_state(psi, r, v)
+        g.run(303, dt)
+        o.run(303, dt)
+        assert_state_parity(g, o, "128^3 step 303", psi_tol=1e-9)
+        with pytest.raises(pkg.He4Error) as ei:
+            g.run(20, dt)
+        assert ei.value.code == pkg.abi.HE4_E_NONFINITE
+        o.run(20, dt)
+        _, ro, vo, _ = o.get_state()
+        assert not (np.all(np.isfinite(vo)) and np.max(np.abs(vo)) < 1e6)
+    o.close()
 
 
 def test_ensemble_members_of_the_larger_grids(pkg, ora):
