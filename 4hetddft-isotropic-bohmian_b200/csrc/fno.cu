@@ -180,6 +180,146 @@ __global__ void k_pointwise(const float *__restrict__ x, const uint16_t *__restr
   }
 }
 
+// ---------------------------------------------------------------------------
+// pointwise layers on the tensor cores: y = W x (+ bias, + add, act) for
+// channel counts that are multiples of 16, as BF16 mma.sync (m16n8k16, FP32
+// accumulate).  The weights are BF16 already; each FP32 activation is split
+// into three BF16 pieces x = x0 + x1 + x2 (x0 = bf16(x), x1 = bf16(x - x0),
+// x2 = bf16(x - x0 - x1): 24 significant bits), and W x0 + W x1 + W x2
+// accumulate in FP32, so the layer keeps FP32 accuracy while every product
+// runs on the tensor cores.  TRANS: A = W^T (the input gradient W^T g).
+// A CTA of 4 warps takes tiles of 64 points; warp w owns points 16w..16w+15
+// of the tile (two n8 tiles) and every output channel (MC/16 m16 tiles).
+// ---------------------------------------------------------------------------
+constexpr int kTcPts = 64;
+
+__device__ __forceinline__ uint32_t pack_bf2(float lo, float hi) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int KC, int MC, bool TRANS>
+__global__ void __launch_bounds__(128) k_pointwise_tc(const float *__restrict__ x, const uint16_t *__restrict__ W,
+                                                      const float *__restrict__ bias, const float *__restrict__ add,
+                                                      float *__restrict__ pre, float *__restrict__ y, int64_t P,
+                                                      int64_t ntiles, int act) {
+  constexpr int KS = KC + 8;  // padded row of the B pieces (bank-conflict free fragment loads)
+  __shared__ __align__(16) uint16_t xs[3][kTcPts][KS];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  // A fragments of the whole weight matrix (MC/16 x KC/16 tiles), in registers
+  uint32_t afr[MC / 16][KC / 16][4];
+#pragma unroll
+  for (int mt = 0; mt < MC / 16; mt++)
+#pragma unroll
+    for (int kt = 0; kt < KC / 16; kt++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int m = mt * 16 + g + ((q & 1) ? 8 : 0), k = kt * 16 + 2 * t + ((q & 2) ? 8 : 0);
+        // A[m][k] = W[m][k] (W is [MC][KC]) or W^T: W[k][m] (W is [KC][MC])
+        const uint16_t lo = TRANS ? W[(size_t)k * MC + m] : W[(size_t)m * KC + k];
+        const uint16_t hi = TRANS ? W[(size_t)(k + 1) * MC + m] : W[(size_t)m * KC + k + 1];
+        afr[mt][kt][q] = (uint32_t)lo | ((uint32_t)hi << 16);
+      }
+  const int64_t tiles_per_b = P / kTcPts;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t b = tile / tiles_per_b, p0 = (tile - b * tiles_per_b) * kTcPts;
+    __syncthreads();
+    // the tile's inputs as three BF16 pieces, point-major
+    for (int e = tid; e < KC * kTcPts; e += 128) {
+      const int k = e / kTcPts, p = e - k * kTcPts;
+      const float v = x[(b * KC + k) * P + p0 + p];
+      const __nv_bfloat16 v0 = __float2bfloat16_rn(v);
+      const float r1 = v - __bfloat162float(v0);
+      const __nv_bfloat16 v1 = __float2bfloat16_rn(r1);
+      const __nv_bfloat16 v2 = __float2bfloat16_rn(r1 - __bfloat162float(v1));
+      xs[0][p][k] = __bfloat16_as_ushort(v0);
+      xs[1][p][k] = __bfloat16_as_ushort(v1);
+      xs[2][p][k] = __bfloat16_as_ushort(v2);
+    }
+    __syncthreads();
+    float acc[MC / 16][2][4];
+#pragma unroll
+    for (int mt = 0; mt < MC / 16; mt++)
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[mt][nt][q] = 0.f;
+#pragma unroll
+    for (int pc = 2; pc >= 0; pc--)  // smallest pieces first
+#pragma unroll
+      for (int kt = 0; kt < KC / 16; kt++)
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) {
+          const uint16_t *row = &xs[pc][warp * 16 + nt * 8 + g][kt * 16 + 2 * t];
+          const uint32_t b0 = *reinterpret_cast<const uint32_t *>(row);
+          const uint32_t b1 = *reinterpret_cast<const uint32_t *>(row + 8);
+#pragma unroll
+          for (int mt = 0; mt < MC / 16; mt++) mma_bf16_16816(acc[mt][nt], afr[mt][kt], b0, b1);
+        }
+    // epilogue: bias, skip term, pre-activation, activation
+#pragma unroll
+    for (int mt = 0; mt < MC / 16; mt++)
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+          const int o = mt * 16 + g + hf * 8;
+          const int64_t pp = p0 + warp * 16 + nt * 8 + 2 * t;
+          const int64_t oi = (b * MC + o) * P + pp;
+          float s0 = acc[mt][nt][2 * hf], s1 = acc[mt][nt][2 * hf + 1];
+          if (bias) {
+            const float bb = bias[o];
+            s0 += bb;
+            s1 += bb;
+          }
+          if (add) {
+            const float2 ad = *reinterpret_cast<const float2 *>(add + oi);
+            s0 += ad.x;
+            s1 += ad.y;
+          }
+          if (pre) *reinterpret_cast<float2 *>(pre + oi) = make_float2(s0, s1);
+          *reinterpret_cast<float2 *>(y + oi) = act ? make_float2(gelu(s0), gelu(s1)) : make_float2(s0, s1);
+        }
+  }
+}
+
+static int launched();
+
+// the tensor-core form applies: channel counts of 16 or 32 (register-held
+// weight fragments) and whole 64-point tiles
+static bool pointwise_tc_ok(int kc, int mc, int64_t P) {
+  return (kc == 16 || kc == 32) && (mc == 16 || mc == 32) && P % kTcPts == 0;
+}
+
+static int launch_pointwise_tc(const float *x, const uint16_t *W, const float *bias, const float *add, float *pre,
+                               float *y, int batch, int kc, int mc, int64_t P, int act, bool trans, cudaStream_t s) {
+  const int64_t ntiles = (int64_t)batch * (P / kTcPts);
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)148 * 8);
+#define HE4_PW_TC(KC_, MC_)                                                                                  \
+  if (kc == KC_ && mc == MC_) {                                                                           \
+    if (trans)                                                                                            \
+      k_pointwise_tc<KC_, MC_, true><<<grid, 128, 0, s>>>(x, W, bias, add, pre, y, P, ntiles, act);      \
+    else                                                                                                  \
+      k_pointwise_tc<KC_, MC_, false><<<grid, 128, 0, s>>>(x, W, bias, add, pre, y, P, ntiles, act);     \
+    return launched();                                                                                    \
+  }
+  HE4_PW_TC(16, 16)
+  HE4_PW_TC(16, 32)
+  HE4_PW_TC(32, 16)
+  HE4_PW_TC(32, 32)
+#undef HE4_PW_TC
+  set_error("pointwise tensor-core kernel: channels %d -> %d", kc, mc);
+  return HE4_E_ARG;
+}
+
 __global__ void k_act_bwd(float *__restrict__ g, const float *__restrict__ pre, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     g[i] *= gelu_grad(pre[i]);
@@ -561,6 +701,8 @@ int he4_fno_pointwise(const float *x, const uint16_t *W, const float *bias, cons
     set_error("he4_fno_pointwise: invalid arguments");
     return HE4_E_ARG;
   }
+  if (pointwise_tc_ok(cin, cout, npts))
+    return launch_pointwise_tc(x, W, bias, add, pre, y, batch, cin, cout, npts, act, false, (cudaStream_t)stream);
   const int64_t total = (int64_t)batch * npts;
   FNO_CI_SWITCH(cin, k_pointwise, blocks_for(total), kThreads, 0, (cudaStream_t)stream >>>(x, W, bias, add, pre, y,
                                                                                          batch, cout, npts, act));
@@ -588,8 +730,12 @@ int he4_fno_pointwise_bwd(float *gy, const float *pre, const float *x, const uin
     HE4_TRY(launched());
   }
   if (gx) {
-    FNO_CI_SWITCH(cout, k_pointwise_gx, blocks_for(total), kThreads, 0, s >>>(gy, W, gx, batch, cin, npts));
-    HE4_TRY(launched());
+    if (pointwise_tc_ok(cout, cin, npts)) {
+      HE4_TRY(launch_pointwise_tc(gy, W, nullptr, nullptr, nullptr, gx, batch, cout, cin, npts, 0, true, s));
+    } else {
+      FNO_CI_SWITCH(cout, k_pointwise_gx, blocks_for(total), kThreads, 0, s >>>(gy, W, gx, batch, cin, npts));
+      HE4_TRY(launched());
+    }
   }
   if (gW || gbias) {
     k_pointwise_wgrad<<<kWgBlocks, kThreads, 0, s>>>(gy, x, work, batch, cin, cout, npts);

@@ -22,8 +22,8 @@ def rel(a, b):
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-30))
 
 
-def make(pkg, seed=3):
-    spec = pkg.fno.FnoSpec(n=16, width=8, modes=(4, 4, 4), layers=3)
+def make(pkg, seed=3, width=8):
+    spec = pkg.fno.FnoSpec(n=16, width=width, modes=(4, 4, 4), layers=3)
     p = pkg.fno.init_params(spec, seed)
     for k in p:
         if k.startswith("R"):
@@ -37,9 +37,12 @@ def oracle_params(net):
     return {k: (wm[k] if k.endswith("_b") or (k.startswith("b") and k[1:].isdigit()) else wb[k]) for k in wb}
 
 
-def test_fno_forward_backward_against_oracle(pkg):
+@pytest.mark.parametrize("width", [8, 16, 32])
+def test_fno_forward_backward_against_oracle(pkg, width):
+    """width 8: CUDA-core pointwise layers; 16 and 32: the tensor-core
+    layers (BF16 mma.sync with three-piece BF16 activations)."""
     import torch
-    spec, p = make(pkg)
+    spec, p = make(pkg, width=width)
     net = pkg.fno.Fno(spec, p)
     rng = np.random.default_rng(5)
     B = 2
