@@ -12,6 +12,8 @@
 // complex flags swapped, which is how the backward pass runs them.
 #include <cuda_bf16.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
 
 #include "../../include/he4_fno.h"
@@ -291,12 +293,104 @@ __global__ void __launch_bounds__(128) k_pointwise_tc(const float *__restrict__ 
   }
 }
 
+// Weight and bias gradients on the tensor cores: gW = g x^T summed over the
+// points (M = CO output channels, N = CI input channels, K = points), both
+// operands FP32 split into three BF16 pieces and the six products of piece
+// orders a + b <= 2 accumulated in FP32 (the dropped terms are below 2^-24
+// of each product).  Each of kWgBlocks CTAs sums a fixed chunk of whole
+// 64-point tiles and writes its partials in k_pointwise_wgrad's layout
+// (pair o * (CI + 1) + i, the bias at i = CI), so the same fixed-order
+// k_wgrad_finish completes both kernels.
+template <int CI, int CO>
+__global__ void __launch_bounds__(128) k_pointwise_wgrad_tc(const float *__restrict__ g, const float *__restrict__ x,
+                                                            float *__restrict__ part, int64_t P, int64_t ntiles) {
+  constexpr int TS = kTcPts + 8;  // padded point rows
+  __shared__ __align__(16) uint16_t gs[3][CO][TS];
+  __shared__ __align__(16) uint16_t xs[3][CI][TS];
+  __shared__ float graw[CO][kTcPts];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, t = lane & 3;
+  constexpr int MT = CO / 16, NT = CI / 8, TILES = MT * NT, PER_WARP = (TILES + 3) / 4;
+  float acc[PER_WARP][4];
+#pragma unroll
+  for (int q = 0; q < PER_WARP; q++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) acc[q][c] = 0.f;
+  float bacc = 0.f;  // bias gradient of channel tid (tid < CO)
+  const int64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
+  const int64_t t0 = blockIdx.x * per, t1 = (t0 + per < ntiles) ? t0 + per : ntiles;
+  const int64_t tiles_per_b = P / kTcPts;
+  for (int64_t tile = t0; tile < t1; tile++) {
+    const int64_t b = tile / tiles_per_b, p0 = (tile - b * tiles_per_b) * kTcPts;
+    __syncthreads();
+    for (int e = tid; e < (CO + CI) * kTcPts; e += 128) {
+      const int c = e / kTcPts, p = e - c * kTcPts;
+      const bool isg = c < CO;
+      const float v = isg ? g[(b * CO + c) * P + p0 + p] : x[(b * CI + (c - CO)) * P + p0 + p];
+      const __nv_bfloat16 v0 = __float2bfloat16_rn(v);
+      const float r1 = v - __bfloat162float(v0);
+      const __nv_bfloat16 v1 = __float2bfloat16_rn(r1);
+      const __nv_bfloat16 v2 = __float2bfloat16_rn(r1 - __bfloat162float(v1));
+      uint16_t(*dst)[TS] = isg ? gs[0] : xs[0];
+      const int row = isg ? c : c - CO;
+      const size_t plane = isg ? (size_t)CO * TS : (size_t)CI * TS;
+      dst[row][p] = __bfloat16_as_ushort(v0);
+      (&dst[0][0])[plane + row * TS + p] = __bfloat16_as_ushort(v1);
+      (&dst[0][0])[2 * plane + row * TS + p] = __bfloat16_as_ushort(v2);
+      if (isg) graw[c][p] = v;
+    }
+    __syncthreads();
+    if (tid < CO)
+      for (int p = 0; p < kTcPts; p++) bacc += graw[tid][p];
+#pragma unroll
+    for (int q = 0; q < PER_WARP; q++) {
+      const int tl = warp * PER_WARP + q;
+      if (tl >= TILES) break;
+      const int mt = tl / NT, nt = tl % NT;
+#pragma unroll
+      for (int kt = 0; kt < kTcPts / 16; kt++)
+#pragma unroll
+        for (int pa = 2; pa >= 0; pa--)
+#pragma unroll
+          for (int pb = 2 - pa; pb >= 0; pb--) {
+            const uint16_t *ar0 = &gs[pa][mt * 16 + gq][kt * 16 + 2 * t];
+            const uint16_t *ar1 = &gs[pa][mt * 16 + gq + 8][kt * 16 + 2 * t];
+            const uint32_t a[4] = {*reinterpret_cast<const uint32_t *>(ar0), *reinterpret_cast<const uint32_t *>(ar1),
+                                   *reinterpret_cast<const uint32_t *>(ar0 + 8),
+                                   *reinterpret_cast<const uint32_t *>(ar1 + 8)};
+            const uint16_t *br = &xs[pb][nt * 8 + gq][kt * 16 + 2 * t];
+            mma_bf16_16816(acc[q], a, *reinterpret_cast<const uint32_t *>(br),
+                           *reinterpret_cast<const uint32_t *>(br + 8));
+          }
+    }
+  }
+  constexpr int npair = CO * (CI + 1);
+  float *out = part + (int64_t)blockIdx.x * npair;
+#pragma unroll
+  for (int q = 0; q < PER_WARP; q++) {
+    const int tl = warp * PER_WARP + q;
+    if (tl >= TILES) break;
+    const int mt = tl / NT, nt = tl % NT;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int o = mt * 16 + gq + ((c & 2) ? 8 : 0), i = nt * 8 + 2 * t + (c & 1);
+      out[o * (CI + 1) + i] = acc[q][c];
+    }
+  }
+  if (tid < CO) out[tid * (CI + 1) + CI] = bacc;
+}
+
 static int launched();
 
 // the tensor-core form applies: channel counts of 16 or 32 (register-held
 // weight fragments) and whole 64-point tiles
+// HE4_FNO_TENSOR_CORES=0 keeps every layer on the CUDA-core kernels (for
+// comparisons; the results agree to FP32 rounding)
 static bool pointwise_tc_ok(int kc, int mc, int64_t P) {
-  return (kc == 16 || kc == 32) && (mc == 16 || mc == 32) && P % kTcPts == 0;
+  static const bool off = [] {
+    const char *s = getenv("HE4_FNO_TENSOR_CORES");
+    return s && s[0] == '0';
+  }();
+  return !off && (kc == 16 || kc == 32) && (mc == 16 || mc == 32) && P % kTcPts == 0;
 }
 
 static int launch_pointwise_tc(const float *x, const uint16_t *W, const float *bias, const float *add, float *pre,
@@ -738,7 +832,13 @@ int he4_fno_pointwise_bwd(float *gy, const float *pre, const float *x, const uin
     }
   }
   if (gW || gbias) {
-    k_pointwise_wgrad<<<kWgBlocks, kThreads, 0, s>>>(gy, x, work, batch, cin, cout, npts);
+    const int64_t ntiles = (int64_t)batch * (npts / kTcPts);
+    if (pointwise_tc_ok(cin, cout, npts) && cin == 32 && cout == 32)
+      k_pointwise_wgrad_tc<32, 32><<<kWgBlocks, 128, 0, s>>>(gy, x, work, npts, ntiles);
+    else if (pointwise_tc_ok(cin, cout, npts) && cin == 16 && cout == 16)
+      k_pointwise_wgrad_tc<16, 16><<<kWgBlocks, 128, 0, s>>>(gy, x, work, npts, ntiles);
+    else
+      k_pointwise_wgrad<<<kWgBlocks, kThreads, 0, s>>>(gy, x, work, batch, cin, cout, npts);
     HE4_TRY(launched());
     k_wgrad_finish<<<(cout * (cin + 1) + kThreads - 1) / kThreads, kThreads, 0, s>>>(work, gW, gbias, kWgBlocks,
                                                                                     cin, cout);
