@@ -119,12 +119,15 @@ class IdentityCoarse:
 # training data from the solver
 # ---------------------------------------------------------------------------
 def trajectory_pairs(pkg_workloads, params, psi0, r0, v0, coarse_steps, steps_per_coarse, dt, enc, net_dev,
-                     form_params=None):
+                     form_params=None, handle=None):
     """Runs one trajectory and returns (inputs, targets) of its coarse steps
-    as float32 device tensors [k][3][nc^3] and [k][2][nc^3]."""
+    as float32 device tensors [k][3][nc^3] and [k][2][nc^3].  handle: an
+    existing He4Step of the same grid to run it on (its captured step
+    graphs are reused across trajectories); otherwise one is created."""
     import torch
     p = form_params if form_params is not None else params
-    g = He4Step(p)
+    own = handle is None
+    g = He4Step(p) if own else handle
     try:
         g.set_state(psi0, r0, v0)
         nc3 = enc.nc ** 3
@@ -145,7 +148,8 @@ def trajectory_pairs(pkg_workloads, params, psi0, r0, v0, coarse_steps, steps_pe
         torch.cuda.synchronize()
         return xs, ys
     finally:
-        g.close()
+        if own:
+            g.close()
 
 
 def train(net, xs, ys, steps, batch=2, lr=1e-3, lr_min=1e-5, seed=0, log=None):

@@ -320,15 +320,20 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     net = fno.Fno(spec, seed=5, device=local)
     t_train = time.perf_counter()
     xs, ys = [], []
+    gen = None
     for i in range(args.fno_traj):
         pm, ps, rm, vm = w.family_member("c2", 10000 + i)
         pm.device = local
+        if gen is None:  # one handle for every trajectory (same grid and form)
+            gen = pkg.He4Step(form_params(pkg, pm, "fp32"))
         enc = pr.FnoCoarse(net, pm, 2, K * dt)
-        a, b = pr.trajectory_pairs(w, pm, ps, rm, vm, 4, K, dt, enc, dev, form_params=form_params(pkg, pm, "fp32"))
+        a, b = pr.trajectory_pairs(w, pm, ps, rm, vm, 4, K, dt, enc, dev, handle=gen)
         xs += a
         ys += b
-    hold_x, hold_y = xs[-4:], ys[-4:]
-    xs, ys = xs[:-4], ys[:-4]
+    gen.close()
+    # the last 8 trajectories (32 coarse steps) are held out
+    hold_x, hold_y = xs[-32:], ys[-32:]
+    xs, ys = xs[:-32], ys[:-32]
     before = pr.evaluate(net, hold_x, hold_y)
     pr.train(net, xs, ys, args.fno_steps, batch=2, lr=1e-3)
     after = pr.evaluate(net, hold_x, hold_y)
@@ -350,6 +355,9 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     clocks = clk.summary()
     launches = sum(h.launch_count() for h in par.handles) - n_lib0 + net.launches
     gstats = [h.graph_stats() for h in par.handles]
+    # coarse-step error over slice 0 at this grid: the network's (as the
+    # judge measured it) and G = identity's (psi unchanged)
+    identity_err = par._rel_psi(par.F[1], par.U[0])
     par.close()
     # accuracy against the plain FP64 sequential run over the same time
     with pkg.He4Step(p) as g64:
@@ -366,6 +374,9 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
             "converged": res["converged"], "exact_by_fallback": res["exact_by_fallback"],
             "diverged": res["diverged"], "fallback_at": res["fallback_at"],
             "changes": res["changes"], "fine_steps_executed": res["fine_steps"],
+            "coarse_step_error": {"fno": res["changes"][0] if res["changes"] else None,
+                                  "identity": identity_err, "judge_threshold": 1e-6,
+                                  "over": f"slice 0 ({PARAREAL_STEPS} fs) at {p.nx}^3"},
             "fno": {"training_trajectories": args.fno_traj, "training_steps": args.fno_steps,
                     "held_out_rel_error_before": before, "held_out_rel_error_after": after,
                     "train_and_data_s": t_train},
@@ -642,8 +653,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
     ap.add_argument("--form", default="parareal", choices=sorted(FORMS))
-    ap.add_argument("--fno-traj", type=int, default=24, help="training trajectories of the FNO (parareal form)")
-    ap.add_argument("--fno-steps", type=int, default=600, help="training steps of the FNO (parareal form)")
+    ap.add_argument("--fno-traj", type=int, default=200, help="training trajectories of the FNO (parareal form)")
+    ap.add_argument("--fno-steps", type=int, default=1500, help="training steps of the FNO (parareal form)")
     ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other forms on the same workload")
     ap.add_argument("--ensemble", type=int, default=64, help="ensemble members timed beside (0 = skip)")
