@@ -443,7 +443,14 @@ def ensemble_form(pkg, args, local, barrier):
         per_grid.setdefault(f"{m[0].nx}^3", t)
     b.close()
     sim = args.ensemble * K * DT_FS * 1e-3
+    # step-level roofline of the batch: the members' algorithmic bytes per
+    # ensemble step (plain FP64 counting rule) over its time
+    peak, _ = load_peaks()
+    ens_bytes = sum(step_bytes("fp64", m[0].nx * m[0].ny * m[0].nz) for m in ms)
+    ens_gbs = ens_bytes / (batched_s / K) / 1e9
     return {"form": f"batched ensemble of {args.ensemble} systems, graphs of up to 30 ensemble steps per launch",
+            "step_roofline": {"bytes_per_ensemble_step": ens_bytes, "achieved_gbs": ens_gbs, "peak_gbs": peak,
+                              "frac": ens_gbs / peak},
             "members_per_grid": {f"{k}^3": v for k, v in sorted(grids.items())}, "steps": K,
             "value": sim / (batched_s / 3600.0), "unit": "simulated ps/hour (sum over members)",
             "ms_per_ensemble_step": batched_s * 1e3 / K, "unbatched_ms_per_ensemble_step": seq_s * 1e3 / K,
