@@ -545,7 +545,12 @@ int he4_step_pc(he4_handle *hh, double deltat, double err[3], double means[9]) {
     set_error("deltat is not finite");
     return HE4_E_ARG;
   }
-  HE4_TRY(step_pc(h, deltat, h->scal));
+  // the step's captured graph (replayed, or captured on first use) where
+  // graphs are on, as he4_run does
+  if (h->use_graphs && h->nsteps_done >= 3)
+    HE4_TRY(run_pc_graphs(h, 1, deltat, h->scal));
+  else
+    HE4_TRY(step_pc(h, deltat, h->scal));
   HE4_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   HE4_CUDA_TRY(cudaStreamSynchronize(h->stream));
   HE4_TRY(check_kernel_errors(h));

@@ -533,8 +533,9 @@ int run_pc_graphs(Handle *h, int n, double dt, double *dres) {
       h->field_valid = 1;
       h->split_valid = 0;
       h->forces_full = 0;
-      HE4_CUDA_TRY(cudaMemcpyAsync(dres + 12 * (size_t)s, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToDevice,
-                                   h->stream));
+      if (dres + 12 * (size_t)s != h->scal)
+        HE4_CUDA_TRY(cudaMemcpyAsync(dres + 12 * (size_t)s, h->scal, 12 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     h->stream));
     } else {
       h->steps_uncaptured++;
       HE4_TRY(step_pc(h, dt, dres + 12 * (size_t)s));
