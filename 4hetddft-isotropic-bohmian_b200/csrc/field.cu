@@ -456,24 +456,26 @@ constexpr int kStreamTY = HE4_STREAM_TY;
 constexpr int kStreamS = HE4_STREAM_S;
 
 // z planes per CTA: the chunk length whose grid fills the resident CTA
-// slots best (fewest waves on a tie), at least 8 planes per chunk
+// slots best (fewest waves on a tie), at least 4 planes per chunk (small
+// grids: 64^3 has 16 row tiles, so its chunks must be short to give the
+// GPU enough CTAs; the longer z halo they re-read comes from L2)
 static int stream_chunk(int nz, int ytiles, int resident) {
-  int best_zc = nz;
-  double best = -1.0;
+  int zcs[8];
+  double effs[8], best = 0.0;
   for (int w = 1; w <= 8; w++) {
-    int nch = std::min(nz, (w * resident) / ytiles);
-    if (nch < 1) continue;
-    const int zc = (nz + nch - 1) / nch;
-    if (zc < 8 && nch > 1) continue;
+    int nch = std::min(nz, std::max(1, (w * resident) / ytiles));
+    const int zc = std::max(4, (nz + nch - 1) / nch);
     const long ctas = (long)ytiles * ((nz + zc - 1) / zc);
     const long waves = (ctas + resident - 1) / resident;
-    const double eff = (double)ctas / (double)(waves * resident);
-    if (eff > best + 1e-9) {
-      best = eff;
-      best_zc = zc;
-    }
+    zcs[w - 1] = zc;
+    effs[w - 1] = (double)ctas / (double)(waves * resident);
+    best = std::max(best, effs[w - 1]);
   }
-  return best_zc;
+  // the longest chunk (least z halo, longest pipeline) within 2 % of the best fill
+  int pick = nz;
+  for (int w = 0; w < 8; w++)
+    if (effs[w] >= best - 0.02 && (pick == nz || zcs[w] > pick)) pick = zcs[w];
+  return pick;
 }
 
 // resident CTAs of a streamed kernel on the handle's device, with its
