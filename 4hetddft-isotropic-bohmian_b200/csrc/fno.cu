@@ -379,6 +379,103 @@ __global__ void __launch_bounds__(128) k_pointwise_wgrad_tc(const float *__restr
   if (tid < CO) out[tid * (CI + 1) + CI] = bacc;
 }
 
+// The truncated transforms along x (the contiguous axis, inner = 1) as
+// real GEMMs on the tensor cores: C[m][n] (+)= sum_k A[m][k] B[k][n] over
+// the rows m of the activations.
+//  - real in, complex out (Fx and the adjoint GxH): A = x [outer][J],
+//    B[j][2k + c] = (Re, Im) of the DFT matrix entry (k, j); C is the
+//    complex result [outer][K] as 2K interleaved floats;
+//  - complex in, real out (Gx and FxH): A = x [outer][J] complex as 2J
+//    floats, B[2j + c][k] = (Re, -Im) of entry (k, j); C = Re(sum) [outer][K].
+// Both operands are FP32 split into three BF16 pieces and the six piece
+// pairs of order <= 2 accumulate in FP32, so the results keep FP32
+// accuracy.  A CTA of four warps takes 64 rows per tile (warp w: rows
+// 16w..16w+15) and every output column.
+__device__ __forceinline__ void split3_bf16(float v, uint16_t &p0, uint16_t &p1, uint16_t &p2) {
+  const __nv_bfloat16 v0 = __float2bfloat16_rn(v);
+  const float r1 = v - __bfloat162float(v0);
+  const __nv_bfloat16 v1 = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 v2 = __float2bfloat16_rn(r1 - __bfloat162float(v1));
+  p0 = __bfloat16_as_ushort(v0);
+  p1 = __bfloat16_as_ushort(v1);
+  p2 = __bfloat16_as_ushort(v2);
+}
+
+template <int KG, int NN>
+__global__ void __launch_bounds__(128) k_contract_x_tc(const float *__restrict__ x, float *__restrict__ y,
+                                                       const float2 *__restrict__ Am, int64_t rows, int J, int K,
+                                                       int in_real, int acc) {
+  constexpr int KS = KG + 8;
+  __shared__ __align__(16) uint16_t as[3][64][KS];
+  __shared__ __align__(16) uint16_t bs[3][NN][KS];  // B transposed: [n][k]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, t = lane & 3;
+  const int kreal = in_real ? J : 2 * J, nreal = in_real ? 2 * K : K;
+  for (int e = tid; e < NN * KG; e += 128) {
+    const int n = e / KG, k = e % KG;
+    float v = 0.f;
+    if (n < nreal && k < kreal) {
+      if (in_real) {  // B[j = k][2kk + c]
+        const float2 a = Am[(n >> 1) * J + k];
+        v = (n & 1) ? a.y : a.x;
+      } else {  // B[2j + c][kk = n]
+        const float2 a = Am[n * J + (k >> 1)];
+        v = (k & 1) ? -a.y : a.x;
+      }
+    }
+    split3_bf16(v, bs[0][n][k], bs[1][n][k], bs[2][n][k]);
+  }
+  const int64_t ntiles = (rows + 63) / 64;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t r0 = tile * 64;
+    __syncthreads();
+    for (int e = tid; e < 64 * KG; e += 128) {
+      const int r = e / KG, k = e % KG;
+      const float v = (r0 + r < rows && k < kreal) ? x[(r0 + r) * kreal + k] : 0.f;
+      split3_bf16(v, as[0][r][k], as[1][r][k], as[2][r][k]);
+    }
+    __syncthreads();
+    float c[NN / 8][4];
+#pragma unroll
+    for (int nt = 0; nt < NN / 8; nt++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) c[nt][q] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < KG / 16; kt++)
+#pragma unroll
+      for (int pa = 2; pa >= 0; pa--) {
+        const uint16_t *ar0 = &as[pa][warp * 16 + gq][kt * 16 + 2 * t];
+        const uint16_t *ar1 = &as[pa][warp * 16 + gq + 8][kt * 16 + 2 * t];
+        const uint32_t a[4] = {*reinterpret_cast<const uint32_t *>(ar0), *reinterpret_cast<const uint32_t *>(ar1),
+                               *reinterpret_cast<const uint32_t *>(ar0 + 8),
+                               *reinterpret_cast<const uint32_t *>(ar1 + 8)};
+#pragma unroll
+        for (int pb = 2 - pa; pb >= 0; pb--)
+#pragma unroll
+          for (int nt = 0; nt < NN / 8; nt++) {
+            const uint16_t *br = &bs[pb][nt * 8 + gq][kt * 16 + 2 * t];
+            mma_bf16_16816(c[nt], a, *reinterpret_cast<const uint32_t *>(br),
+                           *reinterpret_cast<const uint32_t *>(br + 8));
+          }
+      }
+#pragma unroll
+    for (int nt = 0; nt < NN / 8; nt++)
+#pragma unroll
+      for (int hf = 0; hf < 2; hf++) {
+        const int64_t r = r0 + warp * 16 + gq + hf * 8;
+        const int n = nt * 8 + 2 * t;
+        if (r >= rows || n >= nreal) continue;
+        float2 *dst = reinterpret_cast<float2 *>(y + r * nreal + n);  // nreal even: 8-byte aligned
+        float2 v = make_float2(c[nt][2 * hf], c[nt][2 * hf + 1]);
+        if (acc) {
+          const float2 o = *dst;
+          v.x += o.x;
+          v.y += o.y;
+        }
+        *dst = v;
+      }
+  }
+}
+
 static int launched();
 
 // the tensor-core form applies: channel counts of 16 or 32 (register-held
@@ -743,6 +840,21 @@ int he4_fno_contract(const void *x, void *y, const float *A, int32_t outer, int3
   const int64_t total = (int64_t)outer * K * inner;
   const size_t sm = sizeof(float2) * J * K;
   const float2 *A2 = reinterpret_cast<const float2 *>(A);
+  // along the contiguous axis, real <-> complex: tensor-core GEMMs
+  if (inner == 1 && in_real != out_real && pointwise_tc_ok(16, 16, 64)) {
+    const int kreal = in_real ? J : 2 * J, nreal = in_real ? 2 * K : K;
+    const unsigned grid = (unsigned)std::min<int64_t>(((int64_t)outer + 63) / 64, (int64_t)148 * 8);
+    const float *xf = reinterpret_cast<const float *>(x);
+    float *yf = reinterpret_cast<float *>(y);
+    if (kreal <= 32 && nreal <= 64 && nreal % 2 == 0) {
+      k_contract_x_tc<32, 64><<<grid, 128, 0, s>>>(xf, yf, A2, outer, J, K, in_real, accumulate);
+      return launched();
+    }
+    if (kreal <= 64 && nreal <= 24 && nreal % 2 == 0) {
+      k_contract_x_tc<64, 24><<<grid, 128, 0, s>>>(xf, yf, A2, outer, J, K, in_real, accumulate);
+      return launched();
+    }
+  }
   if (in_real && out_real)
     k_contract<true, true><<<blocks_for(total), kThreads, sm, s>>>(x, y, A2, outer, J, K, inner, accumulate);
   else if (in_real)

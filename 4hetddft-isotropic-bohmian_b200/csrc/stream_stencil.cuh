@@ -8,7 +8,7 @@
 // without holding them in registers.  The x taps wrap inside the full row,
 // the y taps read TY + 2M rows of the plane, the z taps a ring of the last
 // 2M + S planes' centre rows.  Periodic grids only (icon = 8); the row
-// length NX is a template parameter (64, 128, 256 or 512) and TY must
+// length NX is a template parameter (128, 256 or 512) and TY must
 // divide ny.
 //
 // Every wait on an mbarrier is bounded (one second of %globaltimer); a CTA
