@@ -208,6 +208,17 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// x = x0 + x1 + x2 in BF16: 24 significant bits of an FP32 value
+__device__ __forceinline__ void split3_bf16(float v, uint16_t &p0, uint16_t &p1, uint16_t &p2) {
+  const __nv_bfloat16 v0 = __float2bfloat16_rn(v);
+  const float r1 = v - __bfloat162float(v0);
+  const __nv_bfloat16 v1 = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 v2 = __float2bfloat16_rn(r1 - __bfloat162float(v1));
+  p0 = __bfloat16_as_ushort(v0);
+  p1 = __bfloat16_as_ushort(v1);
+  p2 = __bfloat16_as_ushort(v2);
+}
+
 template <int KC, int MC, bool TRANS>
 __global__ void __launch_bounds__(128) k_pointwise_tc(const float *__restrict__ x, const uint16_t *__restrict__ W,
                                                       const float *__restrict__ bias, const float *__restrict__ add,
@@ -307,7 +318,7 @@ __global__ void __launch_bounds__(128) k_pointwise_wgrad_tc(const float *__restr
   constexpr int TS = kTcPts + 8;  // padded point rows
   __shared__ __align__(16) uint16_t gs[3][CO][TS];
   __shared__ __align__(16) uint16_t xs[3][CI][TS];
-  __shared__ float graw[CO][kTcPts];
+  __shared__ float bpart_s[CO][kTcPts];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, t = lane & 3;
   constexpr int MT = CO / 16, NT = CI / 8, TILES = MT * NT, PER_WARP = (TILES + 3) / 4;
   float acc[PER_WARP][4];
@@ -315,32 +326,34 @@ __global__ void __launch_bounds__(128) k_pointwise_wgrad_tc(const float *__restr
   for (int q = 0; q < PER_WARP; q++)
 #pragma unroll
     for (int c = 0; c < 4; c++) acc[q][c] = 0.f;
-  float bacc = 0.f;  // bias gradient of channel tid (tid < CO)
+  // bias gradient partials: thread tid stages point tid % 64 of channels
+  // tid / 64 + 2i of g, and sums them over its tiles
+  constexpr int GI = CO * kTcPts / 128, XI = CI * kTcPts / 128;
+  float bpart[GI];
+#pragma unroll
+  for (int i = 0; i < GI; i++) bpart[i] = 0.f;
   const int64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
   const int64_t t0 = blockIdx.x * per, t1 = (t0 + per < ntiles) ? t0 + per : ntiles;
   const int64_t tiles_per_b = P / kTcPts;
+  const int pp = tid % kTcPts, c0 = tid / kTcPts;
   for (int64_t tile = t0; tile < t1; tile++) {
     const int64_t b = tile / tiles_per_b, p0 = (tile - b * tiles_per_b) * kTcPts;
+    // this tile's values in registers before the barrier, so their loads
+    // overlap the previous tile's products in other warps
+    float gv[GI], xv[XI];
+#pragma unroll
+    for (int i = 0; i < GI; i++) gv[i] = g[(b * CO + c0 + 2 * i) * P + p0 + pp];
+#pragma unroll
+    for (int i = 0; i < XI; i++) xv[i] = x[(b * CI + c0 + 2 * i) * P + p0 + pp];
     __syncthreads();
-    for (int e = tid; e < (CO + CI) * kTcPts; e += 128) {
-      const int c = e / kTcPts, p = e - c * kTcPts;
-      const bool isg = c < CO;
-      const float v = isg ? g[(b * CO + c) * P + p0 + p] : x[(b * CI + (c - CO)) * P + p0 + p];
-      const __nv_bfloat16 v0 = __float2bfloat16_rn(v);
-      const float r1 = v - __bfloat162float(v0);
-      const __nv_bfloat16 v1 = __float2bfloat16_rn(r1);
-      const __nv_bfloat16 v2 = __float2bfloat16_rn(r1 - __bfloat162float(v1));
-      uint16_t(*dst)[TS] = isg ? gs[0] : xs[0];
-      const int row = isg ? c : c - CO;
-      const size_t plane = isg ? (size_t)CO * TS : (size_t)CI * TS;
-      dst[row][p] = __bfloat16_as_ushort(v0);
-      (&dst[0][0])[plane + row * TS + p] = __bfloat16_as_ushort(v1);
-      (&dst[0][0])[2 * plane + row * TS + p] = __bfloat16_as_ushort(v2);
-      if (isg) graw[c][p] = v;
+#pragma unroll
+    for (int i = 0; i < GI; i++) {
+      bpart[i] += gv[i];
+      split3_bf16(gv[i], gs[0][c0 + 2 * i][pp], gs[1][c0 + 2 * i][pp], gs[2][c0 + 2 * i][pp]);
     }
+#pragma unroll
+    for (int i = 0; i < XI; i++) split3_bf16(xv[i], xs[0][c0 + 2 * i][pp], xs[1][c0 + 2 * i][pp], xs[2][c0 + 2 * i][pp]);
     __syncthreads();
-    if (tid < CO)
-      for (int p = 0; p < kTcPts; p++) bacc += graw[tid][p];
 #pragma unroll
     for (int q = 0; q < PER_WARP; q++) {
       const int tl = warp * PER_WARP + q;
@@ -376,7 +389,15 @@ __global__ void __launch_bounds__(128) k_pointwise_wgrad_tc(const float *__restr
       out[o * (CI + 1) + i] = acc[q][c];
     }
   }
-  if (tid < CO) out[tid * (CI + 1) + CI] = bacc;
+  // bias: the 64 partials of each channel summed in point order
+#pragma unroll
+  for (int i = 0; i < GI; i++) bpart_s[c0 + 2 * i][pp] = bpart[i];
+  __syncthreads();
+  if (tid < CO) {
+    float s = 0.f;
+    for (int q = 0; q < kTcPts; q++) s += bpart_s[tid][q];
+    out[tid * (CI + 1) + CI] = s;
+  }
 }
 
 // The truncated transforms along x (the contiguous axis, inner = 1) as
@@ -391,15 +412,6 @@ __global__ void __launch_bounds__(128) k_pointwise_wgrad_tc(const float *__restr
 // pairs of order <= 2 accumulate in FP32, so the results keep FP32
 // accuracy.  A CTA of four warps takes 64 rows per tile (warp w: rows
 // 16w..16w+15) and every output column.
-__device__ __forceinline__ void split3_bf16(float v, uint16_t &p0, uint16_t &p1, uint16_t &p2) {
-  const __nv_bfloat16 v0 = __float2bfloat16_rn(v);
-  const float r1 = v - __bfloat162float(v0);
-  const __nv_bfloat16 v1 = __float2bfloat16_rn(r1);
-  const __nv_bfloat16 v2 = __float2bfloat16_rn(r1 - __bfloat162float(v1));
-  p0 = __bfloat16_as_ushort(v0);
-  p1 = __bfloat16_as_ushort(v1);
-  p2 = __bfloat16_as_ushort(v2);
-}
 
 template <int KG, int NN>
 __global__ void __launch_bounds__(128) k_contract_x_tc(const float *__restrict__ x, float *__restrict__ y,
@@ -540,7 +552,7 @@ __global__ void k_pointwise_gx(const float *__restrict__ g, const uint16_t *__re
 
 // weight and bias gradients: block partials over fixed point ranges, then a
 // fixed-order sum over the blocks
-constexpr int kWgBlocks = 296;
+constexpr int kWgBlocks = 592;  // four 128-thread CTAs per SM for the tensor-core form
 constexpr int kWgTile = 64;
 
 __global__ void k_pointwise_wgrad(const float *__restrict__ g, const float *__restrict__ x, float *__restrict__ part,
