@@ -143,6 +143,9 @@ static int create(const he4_params *pin, Handle *h) {
   {
     const char *s = getenv("HE4_STREAM_STENCILS");
     h->use_stream = (s && s[0] == '0') ? 0 : 1;
+    // HE4_POT4_SPLIT=0: the FP32 form's pot4 stencil sums in FP64 instead
+    const char *q = getenv("HE4_POT4_SPLIT");
+    h->pot4_split = (q && q[0] == '0') ? 0 : 1;
   }
   HE4_CUDA_TRY(cudaSetDevice(h->dev));
   cudaDeviceProp prop;

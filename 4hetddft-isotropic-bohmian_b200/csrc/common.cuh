@@ -262,6 +262,8 @@ struct Handle {
   int64_t graph_captures = 0, steps_uncaptured = 0;  // he4_graph_stats
   // row-streamed (bulk-copy pipelined) stencils where the grid allows them
   int use_stream = 1;
+  // FP32-form pot4 stencil: pointwise assembly in FP32 with split weights
+  int pot4_split = 1;
 };
 
 // kernel-level entry points used by the ABI layer

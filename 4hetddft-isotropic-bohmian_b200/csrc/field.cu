@@ -6,8 +6,11 @@
 // transform) for the whole evaluation; forceimp reuses it, since for the
 // periodic stencils (icon=8) FFT(d_i rho) = i D_i(k) FFT(rho) exactly, D_i
 // being the symbol of the npd-point first-derivative stencil.
+#include <string.h>
+
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 #include "common.cuh"
@@ -520,17 +523,38 @@ static bool stream_ok(const Handle *h) {
          h->ny >= 2 * h->st.m && h->nz >= 2 * h->st.m + 1;
 }
 
+// the first-derivative rows of `st` as SplitTaps; false unless every axis's
+// row is antisymmetric with a zero centre (central periodic stencils)
+static bool split_taps(const Stencil &st, SplitTaps *tp) {
+  const int m = st.m;
+  if (m > 6) return false;
+  memset(tp, 0, sizeof(*tp));
+  for (int ax = 0; ax < 3; ax++) {
+    if (st.w1[ax][m] != 0.0) return false;
+    for (int u = 1; u <= m; u++) {
+      const double w = st.w1[ax][m + u];
+      if (st.w1[ax][m - u] != -w) return false;
+      tp->hi[ax][u - 1] = (float)w;
+      tp->lo[ax][u - 1] = (float)(w - (double)tp->hi[ax][u - 1]);
+    }
+  }
+  return true;
+}
+
 template <typename TI, bool OTC, int M, int NX>
 static bool launch_pot4_stream(Handle *h, const TI *lin, const TI *dcg, const TI *h0, const TI *h1, const TI *h2,
                                const OtArgs &ot) {
   using L = Pot4StreamLayout<TI, OTC, M, kStreamTY, kStreamS, NX>;
-  auto kern = k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX>;
+  SplitTaps tp;
+  const bool fm = std::is_same<TI, float>::value && h->pot4_split && split_taps(h->st, &tp);
+  auto kern = fm ? k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX, std::is_same<TI, float>::value>
+                 : k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX, false>;
   const int res = stream_resident(h, kern, L::total);
   if (res == 0) return false;
   const Geo g = geo(h);
   const int yt = h->ny / kStreamTY, zc = stream_chunk(h->nz, yt, res);
   kern<<<dim3(yt, (h->nz + zc - 1) / zc), 256, L::total, h->stream>>>(lin, h->den, dcg, h0, h1, h2, h->pot4, h->st, g,
-                                                                     ot, zc, &h->gred->err);
+                                                                     ot, zc, &h->gred->err, tp);
   HE4_LAUNCHED(h);
   return true;
 }
@@ -770,7 +794,8 @@ static int field_poten_merged(Handle *h) {
 // field_poten_merged of the FP32-convolution form with float intermediate
 // grids (Handle::real32): the same sequence; dencg, denalf, the gradients,
 // the alpha_s integrals (overwritten by the h_i), s and lin are float, den
-// and pot4 stay double, every pointwise and stencil sum is FP64.
+// and pot4 stay double; the gradient and the alpha_s products sum in FP64,
+// the streamed pot4 assembly in FP32 with split weights (k_pot4_stream, FM).
 static int field_poten_merged_f32(Handle *h) {
   const Geo g = geo(h);
   const size_t N = h->N;

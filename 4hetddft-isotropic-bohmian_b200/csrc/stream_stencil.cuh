@@ -88,15 +88,32 @@ struct Pot4StreamLayout {
                           total = h2 + (OTC ? (size_t)RH * TY * rt : 0);
 };
 
+// Central first-derivative weights w_u (u = 1..M, w_-u = -w_u, w_0 = 0)
+// split into float pieces w_u = hi_u + lo_u (|lo_u| <= 2^-24 |w_u|): the
+// float-math pot4 forms sum_u (hi_u + lo_u) (h(+u) - h(-u)) in FP32, so the
+// weights enter with ~48 significant bits and the differences of
+// neighbouring values round far less than the taps themselves.
+struct SplitTaps {
+  float hi[3][6], lo[3][6];
+};
+
 // pot4 of the merged evaluation (poten.f90:80-92,122-124 with term_alfa's
 // divergence term, term_alfa.f90:110-113): the same arithmetic as
 // k_pot4_merged_z, rows streamed.  Grid: (ny / TY, z chunks of zc planes).
-template <typename TI, bool OTC, int M, int TY, int S, int NX>
+// FM (float grids of the FP32-convolution form, antisymmetric first-
+// derivative rows): the pointwise assembly in FP32 -- the divergence with
+// split weights (SplitTaps), the correlation term from the float dencg, the
+// solid penalty from tanh written through e = exp(-2|x|) (1 + tanh x =
+// 2/(1+e) for x >= 0, 2e/(1+e) below; 1 - tanh^2 x = 4e/(1+e)^2), which
+// also avoids the cancellation of 1 + tanh x for x << 0 -- and only the
+// final three-term sum in FP64.  Five float/double conversions per point
+// instead of 23.
+template <typename TI, bool OTC, int M, int TY, int S, int NX, bool FM = false>
 __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin, const double *__restrict__ den,
                                                      const TI *__restrict__ dencg, const TI *__restrict__ h0,
                                                      const TI *__restrict__ h1, const TI *__restrict__ h2,
                                                      double *__restrict__ pot4, Stencil st, Geo g, OtArgs a, int zc,
-                                                     unsigned *err) {
+                                                     unsigned *err, SplitTaps tp) {
   extern __shared__ __align__(128) unsigned char smem[];
   using L = Pot4StreamLayout<TI, OTC, M, TY, S, NX>;
   constexpr int RH = L::RH, PX = L::PX, RS0 = L::RS0;
@@ -160,6 +177,7 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
   if (warp == 0)
     for (int q = 0; q < S && k0 + q < k1; q++) issue(k0 + q, q, q == 0);
   const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0, adiv = a.h2o2m4 * a.alphas;
+  const float fa0 = (float)a0, fa1 = (float)a1, fcs = (float)a.c_solid, fbeta = (float)a.beta;
   constexpr int NPT = TY * NX;
   for (int k = k0; k < k1; k++) {
     const int it = k - k0, s = it % S;
@@ -186,6 +204,33 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
     for (int p = tid; p < NPT; p += 256) {
       const int r = p / NX, x = p % NX;
       const double d = dd[p];
+      if constexpr (FM) {
+        const float xs = (float)(a.beta * (d - a.den_m)), df = (float)d;
+        const float e = expf(-2.0f * fabsf(xs)), q = 1.0f / (1.0f + e);
+        const float opt = (xs >= 0.0f ? 2.0f : 2.0f * e) * q, omt = 4.0f * e * q * q;
+        const float dc = cc[p];
+        const float cp = dc * dc * (fa0 + fa1 * dc) + fcs * (opt + fbeta * df * omt);
+        double v = (double)ll[p] + (double)cp;
+        if (OTC) {
+          const TI *xr = x0 + r * RS0 + x;
+          const TI *yc = y1 + r * NX + x;
+          float sh = 0.0f, sl = 0.0f;
+#pragma unroll
+          for (int u = M; u >= 1; u--) {
+            const float ex = xr[u] - xr[-u], ey = yc[(M + u) * NX] - yc[(M - u) * NX],
+                        ez = zr[M + u][p] - zr[M - u][p];
+            sh = fmaf(tp.hi[0][u - 1], ex, sh);
+            sl = fmaf(tp.lo[0][u - 1], ex, sl);
+            sh = fmaf(tp.hi[1][u - 1], ey, sh);
+            sl = fmaf(tp.lo[1][u - 1], ey, sl);
+            sh = fmaf(tp.hi[2][u - 1], ez, sh);
+            sl = fmaf(tp.lo[2][u - 1], ez, sl);
+          }
+          v += (double)(sh + sl) * adiv;
+        }
+        out[p] = v;
+        continue;
+      }
       const double th = tanh(a.beta * (d - a.den_m));
       const double pen = a.c_solid * (1.0 + th + a.beta * d * (1.0 - th * th));
       const double dc = (double)cc[p];
