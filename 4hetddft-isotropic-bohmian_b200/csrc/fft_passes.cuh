@@ -5,6 +5,8 @@
 #pragma once
 #include <cuda_pipeline.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft_reg.cuh"
 
@@ -121,6 +123,24 @@ __device__ __forceinline__ double xload(const XLoad &ld, const TI *__restrict__ 
     return d * c * (ld.c0 + ld.c1 * c);
   }
   return (double)in[i];
+}
+
+// the same element as the spectrum's scalar T; with float spectra and float
+// grids the source is formed in FP32 (float <-> double conversions run at a
+// quarter of the FP64 rate on this GPU, and the spectrum keeps 24 bits
+// anyway); c0f / c1f are ld.c0 / ld.c1 rounded to float once per thread
+template <int OP, typename TI, typename T>
+__device__ __forceinline__ T xload_t(const XLoad &ld, const TI *__restrict__ in, long i, float c0f, float c1f) {
+  if constexpr (std::is_same<T, float>::value && std::is_same<TI, float>::value) {
+    if (OP == XLOAD_ALFA) return fmaf(-static_cast<const float *>(ld.aux0)[i], c0f, 1.0f) * in[i];
+    if (OP == XLOAD_CORR) {
+      const float d = (float)static_cast<const double *>(ld.aux0)[i], c = static_cast<const float *>(ld.aux1)[i];
+      return d * c * fmaf(c1f, c, c0f);
+    }
+    return in[i];
+  } else {
+    return (T)xload<OP, TI>(ld, in, i);
+  }
 }
 
 template <int N, typename C2>
@@ -397,17 +417,18 @@ __global__ void __launch_bounds__(kRegThreads) k_xr2c_reg(XRegArgs<C2> a) {
   // loads from clamped rows (unconditional, so they issue together), rows
   // past the end zeroed afterwards
   const long rac = ra < a.nrow ? ra : a.nrow - 1, rbc = rb < a.nrow ? rb : a.nrow - 1;
-  double xa[N2], xb[N2];
+  const float c0f = (float)a.ld.c0, c1f = (float)a.ld.c1;
+  T xa[N2], xb[N2];
 #pragma unroll
   for (int j2 = 0; j2 < N2; j2++) {
     const int x = j1 + N1 * j2;
-    xa[j2] = xload<OP, TI>(a.ld, in, rac * N + x);
-    xb[j2] = xload<OP, TI>(a.ld, in, rbc * N + x);
+    xa[j2] = xload_t<OP, TI, T>(a.ld, in, rac * N + x, c0f, c1f);
+    xb[j2] = xload_t<OP, TI, T>(a.ld, in, rbc * N + x, c0f, c1f);
   }
   C2 v[N2];
 #pragma unroll
   for (int j2 = 0; j2 < N2; j2++)
-    v[j2] = regfft::mk<C2>((T)((ra < a.nrow) ? xa[j2] : 0.0), (T)((rb < a.nrow) ? xb[j2] : 0.0));
+    v[j2] = regfft::mk<C2>((ra < a.nrow) ? xa[j2] : T(0), (rb < a.nrow) ? xb[j2] : T(0));
   regfft::LayoutX lay{p * SP};
   regfft::fwd2<N, N1, false>(v, S, lay, j1, tw);
   C2 *Sp = S + p * SP;
@@ -471,11 +492,23 @@ __global__ void __launch_bounds__(kRegThreads) k_xc2r_reg(XRegArgs<C2> a) {
   regfft::LayoutX lay{p * SP};
   regfft::bwd2<N, N1, true>(v, S, lay, j1, tw);
   const double sc = a.scale;
+  if constexpr (std::is_same<TO, float>::value && std::is_same<C2, float2>::value) {
+    // float spectra into float grids: no double round trip (the same
+    // result whenever the scale is a power of two, as the callers' 1.0 is)
+    const float scf = (float)sc;
 #pragma unroll
-  for (int n2 = 0; n2 < N2; n2++) {
-    const int x = j1 + N1 * n2;
-    if (ina) out[ra * N + x] = (TO)((double)v[n2].x * sc);
-    if (inb) out[rb * N + x] = (TO)((double)v[n2].y * sc);
+    for (int n2 = 0; n2 < N2; n2++) {
+      const int x = j1 + N1 * n2;
+      if (ina) out[ra * N + x] = v[n2].x * scf;
+      if (inb) out[rb * N + x] = v[n2].y * scf;
+    }
+  } else {
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) {
+      const int x = j1 + N1 * n2;
+      if (ina) out[ra * N + x] = (TO)((double)v[n2].x * sc);
+      if (inb) out[rb * N + x] = (TO)((double)v[n2].y * sc);
+    }
   }
 }
 
