@@ -557,8 +557,10 @@ constexpr int kWgTile = 64;
 
 __global__ void k_pointwise_wgrad(const float *__restrict__ g, const float *__restrict__ x, float *__restrict__ part,
                                   int B, int ci, int co, int64_t P) {
-  __shared__ float sx[kMaxCh][kWgTile];
-  __shared__ float sg[kMaxCh][kWgTile];
+  // rows padded by one: the threads of a warp read different channels at
+  // the same point, which an unpadded 64-float pitch maps to one bank
+  __shared__ float sx[kMaxCh][kWgTile + 1];
+  __shared__ float sg[kMaxCh][kWgTile + 1];
   const int npair = co * (ci + 1);
   const int64_t total = (int64_t)B * P;
   const int64_t chunk = (total + gridDim.x - 1) / gridDim.x;
@@ -604,12 +606,19 @@ __global__ void k_pointwise_wgrad(const float *__restrict__ g, const float *__re
   }
 }
 
+// one warp per (output, input or bias) pair: lane l sums the partials of
+// blocks l, l + 32, ... in FP64, then a fixed shuffle tree adds the lanes,
+// so the order (and the result) is the same on every run
 __global__ void k_wgrad_finish(const float *__restrict__ part, float *__restrict__ gW, float *__restrict__ gb,
                                int nblk, int ci, int co) {
   const int npair = co * (ci + 1);
-  for (int pr = blockIdx.x * blockDim.x + threadIdx.x; pr < npair; pr += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  for (int pr = blockIdx.x * wpb + (threadIdx.x >> 5); pr < npair; pr += gridDim.x * wpb) {
     double s = 0.0;
-    for (int b = 0; b < nblk; b++) s += (double)part[(int64_t)b * npair + pr];
+    for (int b = lane; b < nblk; b += 32) s += (double)part[(int64_t)b * npair + pr];
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+    if (lane != 0) continue;
     const int o = pr / (ci + 1), i = pr % (ci + 1);
     if (i < ci) {
       if (gW) gW[o * ci + i] = (float)s;
@@ -964,8 +973,8 @@ int he4_fno_pointwise_bwd(float *gy, const float *pre, const float *x, const uin
     else
       k_pointwise_wgrad<<<kWgBlocks, kThreads, 0, s>>>(gy, x, work, batch, cin, cout, npts);
     HE4_TRY(launched());
-    k_wgrad_finish<<<(cout * (cin + 1) + kThreads - 1) / kThreads, kThreads, 0, s>>>(work, gW, gbias, kWgBlocks,
-                                                                                    cin, cout);
+    const int wpb = kThreads / 32;  // one warp per pair
+    k_wgrad_finish<<<(cout * (cin + 1) + wpb - 1) / wpb, kThreads, 0, s>>>(work, gW, gbias, kWgBlocks, cin, cout);
     HE4_TRY(launched());
   }
   return HE4_OK;
