@@ -268,9 +268,10 @@ int he4_device_ptr(he4_handle *h, int32_t which, void **ptr);
  * kernels inside the graph). */
 int64_t he4_launch_count(he4_handle *h);
 /* CUDA-graph use of he4_run: how many PC-step graphs the handle captured
- * (one per distinct buffer rotation of the step, at most 24) and how many
- * PC steps ran uncaptured (launched one kernel at a time) because no
- * captured graph matched.  Has no counterpart in the reference. */
+ * (one per distinct buffer rotation of the step; the rotations repeat every
+ * 30 steps) and how many PC steps ran uncaptured (launched one kernel at a
+ * time) because no captured graph matched.  Has no counterpart in the
+ * reference. */
 int he4_graph_stats(he4_handle *h, int64_t *captured, int64_t *uncaptured);
 
 /* Tile shapes of the FFT passes: tiles = {n1 x, n1 y, n1 z, px, wy, wz}.
