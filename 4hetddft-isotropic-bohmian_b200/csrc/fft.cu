@@ -775,6 +775,16 @@ const double *dsym_of<double2>(const Handle *h) { return h->dsym; }
 template <>
 const float *dsym_of<float2>(const Handle *h) { return h->dsym32; }
 
+// HE4_ZCONV_SHARE_XY=0 transforms the x and y force outputs separately (for
+// comparisons; equal to rounding)
+static bool share_xy_on() {
+  static const bool on = [] {
+    const char *e = getenv("HE4_ZCONV_SHARE_XY");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // register-path fused z pass: consecutive operations on the same input share
 // one forward transform
 template <typename C2>
@@ -798,8 +808,28 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
       return HE4_E_ARG;
     }
     ZGroupT<C2> &g = groups[ng - 1];
+    g.xy_shared = 0;
     g.o[g.nout++] = ZOutT<C2>{reinterpret_cast<C2 *>(ops[i].out), kern_of<C2>(h, ops[i].kern), ops[i].coef,
                               ops[i].dsym_axis, ops[i].boxz};
+  }
+  // the three derivative outputs of one kernel (the force field): ordered
+  // z, x, y so that the x and y outputs share one inverse transform
+  for (int i = 0; i < ng; i++) {
+    ZGroupT<C2> &g = groups[i];
+    if (g.nout != 3 || !share_xy_on()) continue;
+    int at[3] = {-1, -1, -1};
+    bool same = true;
+    for (int o = 0; o < 3; o++) {
+      const ZOutT<C2> &z = g.o[o];
+      same = same && z.kern == g.o[0].kern && z.coef == g.o[0].coef && z.boxz == g.o[0].boxz;
+      if (z.dsym_axis >= 0 && z.dsym_axis < 3) at[z.dsym_axis] = o;
+    }
+    if (!same || at[0] < 0 || at[1] < 0 || at[2] < 0) continue;
+    const ZOutT<C2> oz = g.o[at[2]], ox = g.o[at[0]], oy = g.o[at[1]];
+    g.o[0] = oz;
+    g.o[1] = ox;
+    g.o[2] = oy;
+    g.xy_shared = 1;
   }
   for (int g0 = 0; g0 < ng; g0 += kMaxBatch) {
     const int nb = std::min(kMaxBatch, ng - g0);

@@ -74,6 +74,12 @@ template <typename C2>
 struct ZGroupT {
   const C2 *in;
   int nout;
+  // xy_shared: three outputs with one kernel and coefficient and the
+  // derivative symbols of axes z, x, y in that order.  D_x(kx) and D_y(ky)
+  // are constant along a z pencil, so the x and y outputs are
+  // i D IFFT_z(coef K X): the x output's inverse transform also writes the
+  // y output, and the kernels run two transforms instead of three
+  int xy_shared;
   ZOutT<C2> o[kMaxOut];
 };
 
@@ -241,7 +247,8 @@ __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
   }
   __syncthreads();
   const ZGroupT<C2> &G = a.g[blockIdx.x];
-  const int nout = SINGLE ? 1 : G.nout;
+  const bool xys = !SINGLE && G.xy_shared;
+  const int nout = SINGLE ? 1 : (xys ? 2 : G.nout);
   auto prefetch = [&](int o) {
     const T *kern = G.o[o].kern;
     if (!kern) return;
@@ -281,7 +288,7 @@ __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
         T cf = coef;
         if (Z.kern && off >= 0) cf *= K[k * W + w];
         C2 y = regfft::scale(v[c * N1 + k1], cf);
-        if (Z.dsym_axis >= 0) {
+        if (Z.dsym_axis >= 0 && !(xys && o == 1)) {
           const T ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
           y = regfft::mk<C2>(-y.y * ds, y.x * ds);
         }
@@ -291,10 +298,22 @@ __global__ void __launch_bounds__(kRegThreads) k_zconv_reg(ZRegArgs<C2> a) {
     if (off >= 0) {
       int zlo = 0, zhi = N - 1;
       if (Z.boxz) force_range(a.box, 2, a.nz, &zlo, &zhi);
+      if (xys && o == 1) {  // x and y outputs: i D_x and i D_y times the transform
+        C2 *oy = G.o[2].out;
 #pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) {
-        const int z = j1 + N1 * n2;
-        if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+        for (int n2 = 0; n2 < N2; n2++) {
+          const int z = j1 + N1 * n2;
+          if (z >= zlo && z <= zhi) {
+            Z.out[off + z * a.sf] = regfft::mk<C2>(-x[n2].y * dx, x[n2].x * dx);
+            oy[off + z * a.sf] = regfft::mk<C2>(-x[n2].y * dy, x[n2].x * dy);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) {
+          const int z = j1 + N1 * n2;
+          if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+        }
       }
     }
   }
@@ -314,7 +333,8 @@ __global__ void __launch_bounds__(kRegThreads, sizeof(C2) == 8 ? 2 : 1) k_zconv_
   load_tw_n<N>(tw, a.tw);
   __syncthreads();
   const ZGroupT<C2> &G = a.g[blockIdx.x];
-  const int nout = SINGLE ? 1 : G.nout;
+  const bool xys = !SINGLE && G.xy_shared;
+  const int nout = SINGLE ? 1 : (xys ? 2 : G.nout);
   const int w = threadIdx.x % W, j1 = threadIdx.x / W;
   const long ntiles = (a.map.nxh * (long)a.map.nother + W - 1) / W;
   auto pencil = [&](long tile, int *kx, int *ky) -> long {
@@ -366,7 +386,7 @@ __global__ void __launch_bounds__(kRegThreads, sizeof(C2) == 8 ? 2 : 1) k_zconv_
           T cf = coef;
           if (Z.kern && off >= 0) cf *= K[c * N1 + k1];
           C2 y = regfft::scale(v[c * N1 + k1], cf);
-          if (Z.dsym_axis >= 0) {
+          if (Z.dsym_axis >= 0 && !(xys && o == 1)) {
             const T ds = (Z.dsym_axis == 0) ? dx : (Z.dsym_axis == 1) ? dy : a.dsym[a.nx + a.ny + k];
             y = regfft::mk<C2>(-y.y * ds, y.x * ds);
           }
@@ -376,10 +396,22 @@ __global__ void __launch_bounds__(kRegThreads, sizeof(C2) == 8 ? 2 : 1) k_zconv_
       if (off >= 0) {
         int zlo = 0, zhi = N - 1;
         if (Z.boxz) force_range(a.box, 2, a.nz, &zlo, &zhi);
+        if (xys && o == 1) {  // x and y outputs: i D_x and i D_y times the transform
+          C2 *oy = G.o[2].out;
 #pragma unroll
-        for (int n2 = 0; n2 < N2; n2++) {
-          const int z = j1 + N1 * n2;
-          if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+          for (int n2 = 0; n2 < N2; n2++) {
+            const int z = j1 + N1 * n2;
+            if (z >= zlo && z <= zhi) {
+              Z.out[off + z * a.sf] = regfft::mk<C2>(-x[n2].y * dx, x[n2].x * dx);
+              oy[off + z * a.sf] = regfft::mk<C2>(-x[n2].y * dy, x[n2].x * dy);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int n2 = 0; n2 < N2; n2++) {
+            const int z = j1 + N1 * n2;
+            if (z >= zlo && z <= zhi) Z.out[off + z * a.sf] = x[n2];
+          }
         }
       }
       if (!SINGLE) {
