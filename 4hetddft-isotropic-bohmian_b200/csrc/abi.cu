@@ -146,6 +146,9 @@ static int create(const he4_params *pin, Handle *h) {
     // HE4_POT4_SPLIT=0: the FP32 form's pot4 stencil sums in FP64 instead
     const char *q = getenv("HE4_POT4_SPLIT");
     h->pot4_split = (q && q[0] == '0') ? 0 : 1;
+    // HE4_ZCONV_SHARE_XY=0: the x and y force outputs transformed separately
+    const char *z = getenv("HE4_ZCONV_SHARE_XY");
+    h->zconv_share_xy = (z && z[0] == '0') ? 0 : 1;
   }
   HE4_CUDA_TRY(cudaSetDevice(h->dev));
   cudaDeviceProp prop;

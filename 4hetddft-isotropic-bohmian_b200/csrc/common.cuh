@@ -264,6 +264,8 @@ struct Handle {
   int use_stream = 1;
   // FP32-form pot4 stencil: pointwise assembly in FP32 with split weights
   int pot4_split = 1;
+  // force z convolution: one inverse transform for the x and y outputs
+  int zconv_share_xy = 1;
 };
 
 // kernel-level entry points used by the ABI layer

@@ -775,16 +775,6 @@ const double *dsym_of<double2>(const Handle *h) { return h->dsym; }
 template <>
 const float *dsym_of<float2>(const Handle *h) { return h->dsym32; }
 
-// HE4_ZCONV_SHARE_XY=0 transforms the x and y force outputs separately (for
-// comparisons; equal to rounding)
-static bool share_xy_on() {
-  static const bool on = [] {
-    const char *e = getenv("HE4_ZCONV_SHARE_XY");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
 // register-path fused z pass: consecutive operations on the same input share
 // one forward transform
 template <typename C2>
@@ -816,7 +806,7 @@ static int zconv_reg(Handle *h, int n, const ZOp *ops) {
   // z, x, y so that the x and y outputs share one inverse transform
   for (int i = 0; i < ng; i++) {
     ZGroupT<C2> &g = groups[i];
-    if (g.nout != 3 || !share_xy_on()) continue;
+    if (g.nout != 3 || !h->zconv_share_xy) continue;
     int at[3] = {-1, -1, -1};
     bool same = true;
     for (int o = 0; o < 3; o++) {

@@ -331,6 +331,7 @@ class Parareal:
         run, so speculation only pays when one iteration converges."""
         torch = self.torch
         max_iter = self.S if max_iter is None else max_iter
+        self.fine_steps = 0  # counted per run
         t0 = time.perf_counter()
         self.U[0].psi.copy_(torch.from_numpy(np.ascontiguousarray(psi0).view(np.float64).reshape(
             self.U[0].psi.shape)))

@@ -266,8 +266,9 @@ def gpu_arm(args):
     if rank != 0:
         return
     timed = ("K predictor-corrector steps from device-resident state (he4_run); K = --steps" if par is None else
-             f"a fixed {PARAREAL_SLICES} x {PARAREAL_STEPS} fs of parareal from device-resident state (FNO "
-             f"training untimed); --steps K sets the K PC steps each step form in 'forms' times")
+             f"a fixed {PARAREAL_SLICES} x {PARAREAL_STEPS} fs of parareal from device-resident state, the "
+             f"median of {args.parareal_reps} runs (FNO training untimed); --steps K sets the K PC steps each "
+             f"step form in 'forms' times")
     line = {
         "metric": METRIC,
         "value": value,
@@ -342,18 +343,29 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     coarse = pr.FnoCoarse(net, q, p.nx // spec.n, K * dt)
     par = pr.Parareal(q, S, K, dt, coarse, concurrent=8)
     par.warm(psi, r, v)  # graph capture of the fine propagators, untimed
-    n_lib0 = sum(h.launch_count() for h in par.handles)
-    barrier()
+    # the whole run is one timed region of ~1.5 s, so one stall of the shared
+    # host or GPU moves it far; it is repeated from the same state and the
+    # median run is reported (every run's time is listed)
+    runs = []
     with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
-        res = par.run(psi, r, v, tol=1e-6)
-        fin = par.final_state()
-        psi_out = fin.psi.cpu().numpy().view(np.complex128).reshape(psi.shape)
-        r_out = fin.r.cpu().numpy()
-        v_out = fin.v.cpu().numpy()
-        e2e_s = time.perf_counter() - t0
+        for _ in range(max(1, args.parareal_reps)):
+            n_lib0 = sum(h.launch_count() for h in par.handles)
+            n_net0 = net.launches
+            barrier()
+            t0 = time.perf_counter()
+            res = par.run(psi, r, v, tol=1e-6)
+            fin = par.final_state()
+            psi_out = fin.psi.cpu().numpy().view(np.complex128).reshape(psi.shape)
+            r_out = fin.r.cpu().numpy()
+            v_out = fin.v.cpu().numpy()
+            e2e_s = time.perf_counter() - t0
+            launches = sum(h.launch_count() for h in par.handles) - n_lib0 + (net.launches - n_net0)
+            runs.append((res["device_s"], e2e_s, res, launches, psi_out, r_out, v_out))
     clocks = clk.summary()
-    launches = sum(h.launch_count() for h in par.handles) - n_lib0 + net.launches
+    device_runs = [x[0] for x in runs]
+    e2e_runs = [x[1] for x in runs]
+    _, _, res, launches, psi_out, r_out, v_out = sorted(runs, key=lambda x: x[0])[len(runs) // 2]
+    e2e_s = float(np.median(e2e_runs))
     gstats = [h.graph_stats() for h in par.handles]
     # coarse-step error over slice 0 at this grid: the network's (as the
     # judge measured it) and G = identity's (psi unchanged)
@@ -370,6 +382,8 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     d64, dpar = np.abs(psi64) ** 2, np.abs(psi_out) ** 2
     sim_ps = S * K * DT_FS * 1e-3
     return {"form": FORMS["parareal"], "sim_ps": sim_ps, "device_s": res["device_s"], "e2e_s": e2e_s,
+            "runs": {"count": len(runs), "device_s": device_runs, "e2e_s": e2e_runs,
+                     "reported": "median run (device time); e2e is the median of the runs' e2e times"},
             "iterations": res["iterations"],
             "converged": res["converged"], "exact_by_fallback": res["exact_by_fallback"],
             "diverged": res["diverged"], "fallback_at": res["fallback_at"],
@@ -662,6 +676,8 @@ def main():
     ap.add_argument("--form", default="parareal", choices=sorted(FORMS))
     ap.add_argument("--fno-traj", type=int, default=200, help="training trajectories of the FNO (parareal form)")
     ap.add_argument("--fno-steps", type=int, default=1500, help="training steps of the FNO (parareal form)")
+    ap.add_argument("--parareal-reps", type=int, default=3,
+                    help="timed parareal runs from the same state; the median is reported")
     ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other forms on the same workload")
     ap.add_argument("--ensemble", type=int, default=64, help="ensemble members timed beside (0 = skip)")

@@ -401,3 +401,21 @@ def test_launch_count_and_errors(pkg, c1):
         assert g.launch_count() > n0
         with pytest.raises(pkg.He4Error):
             g.steppc(float("nan"))
+
+
+def test_force_xy_shared_transform(pkg, monkeypatch):
+    """The force z convolution transforms i D_x and i D_y once (they are
+    constant along z); HE4_ZCONV_SHARE_XY=0 transforms each output.  The
+    full-grid forces agree to FP64 rounding."""
+    w = pkg.workloads
+    p, psi, r, v, _ = w.workload("c1")
+    f = {}
+    for share in ("1", "0"):
+        monkeypatch.setenv("HE4_ZCONV_SHARE_XY", share)
+        with pkg.He4Step(p) as g:
+            g.set_state(psi, r, v)
+            g.field()
+            f[share] = [g.get_field(n) for n in ("fx", "fy", "fz")]
+    for a, b in zip(f["1"], f["0"]):
+        scale = np.max(np.abs(b))
+        assert np.max(np.abs(a - b)) <= 1e-12 * scale
