@@ -778,7 +778,7 @@ int he4_fft_c2r(he4_handle *hh, const double *in, double *out) {
   return HE4_OK;
 }
 
-constexpr int kBenchKernels = 12;
+constexpr int kBenchKernels = 13;
 
 static int launch_bench(Handle *h, int which) {
   switch (which) {
@@ -808,6 +808,10 @@ static int launch_bench(Handle *h, int which) {
     case 9: return launch_pot4_merged_f32(h);
     case 10: return fft_x_c2r_f32_only(h, h->spec[1], h->g32[8]);
     case 11: return launch_grad_f32(h);
+    case 12: {
+      double2 *b[1] = {h->spec[1]};
+      return fft_y(h, 1, b, true);
+    }
     default: set_error("unknown kernel id %d", which); return HE4_E_ARG;
   }
 }
@@ -826,7 +830,7 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
       "k_xc2r_reg (x C2R)",         "k_zconv (z pass, no multiply)", "k_zconv (z conv, no kernel)",
       "k_zconv (z conv, 3 outputs)", "k_grad_z (density gradient)",  "k_pot4_merged_z (pot4, FP64 grids)",
       "k_pot4_merged_z (pot4, float grids)", "k_xc2r_reg (x C2R, float rows)",
-      "k_grad_z (density gradient, float grids)"};
+      "k_grad_z (density gradient, float grids)", "k_yz_pipe (y pass, inverse)"};
   const double H = (double)h->H, N = (double)h->N;
   // algorithmic bytes: read input once, write output once (+ the real
   // kernel); c and k are the sizes of a spectrum and a kernel element
@@ -841,7 +845,9 @@ int he4_bench_kernel(he4_handle *hh, int32_t which, int32_t reps, double *ms_per
       // half spectrum in, float rows out
       c * H + 4 * N,
       // den in, three float gradients out
-      8 * N + 3 * 4 * N};
+      8 * N + 3 * 4 * N,
+      // inverse y pass, in place
+      2 * c * H};
   if (which < 0 || which >= kBenchKernels) {
     set_error("unknown kernel id %d", which);
     return HE4_E_ARG;

@@ -218,6 +218,7 @@ def gpu_arm(args):
         forms[form]["step_roofline"] = {"bytes_per_step": sb, "achieved_gbs": sb / (ms_step * 1e-3) / 1e9,
                                         "peak_gbs": peak, "frac": sb / (ms_step * 1e-3) / 1e9 / peak}
         forms[form]["roofline"] = kernel_roofline(pkg, gf, args, form)
+        forms[form]["kernels"] = [kernel_roofline(pkg, gf, args, form, which=i) for i in NEXT_KERNELS[form]]
         forms[form]["e2e"] = e2e_leg(pkg, torch, gf, psi, r, v, dt, args, barrier, dist, local, world)
         if form == step_form:
             g, stream = gf, sf
@@ -478,8 +479,11 @@ def pin(torch, a):
 
 
 # dominant kernel of each step form's launch list (profiles/launch_list_*):
-# he4_bench_kernel ids 9 (merged pot4 on float grids) and 3 (x pass C2R)
-DOMINANT_KERNEL = {"fp32": 9, "fp64": 3}
+# he4_bench_kernel ids 12 (inverse y pass) and 3 (x pass C2R); the next
+# kernels of each list are timed beside it (ids 6: z convolution with three
+# outputs, 9: merged pot4 on float grids, 8: on FP64 grids, 1: forward y pass)
+DOMINANT_KERNEL = {"fp32": 12, "fp64": 3}
+NEXT_KERNELS = {"fp32": (6, 9), "fp64": (1, 6, 8)}
 
 
 def step_bytes(form, n):
@@ -495,17 +499,17 @@ def step_bytes(form, n):
     return (1256 if form == "fp32" else 1720) * float(n)
 
 
-def kernel_roofline(pkg, g, args, form, reps=20):
-    """Average duration of the form's dominant kernel, timed with CUDA
-    events on the library's stream (the kernel's own launch stream), against
-    its algorithmic bytes; DRAM traffic per launch from the committed ncu
-    capture of the same kernel."""
+def kernel_roofline(pkg, g, args, form, reps=20, which=None):
+    """Average duration of the form's dominant kernel (or of bench id
+    `which`), timed with CUDA events on the library's stream (the kernel's
+    own launch stream), against its algorithmic bytes; DRAM traffic per
+    launch from the committed ncu capture of the same kernel."""
     L = pkg.load_library()
     L.he4_bench_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double), C.c_char_p, C.c_int32]
     ms, byts = C.c_double(), C.c_double()
     name = C.create_string_buffer(64)
-    which = DOMINANT_KERNEL[form]
+    which = DOMINANT_KERNEL[form] if which is None else which
     g.field()  # the stencil ids work on the fields of a current evaluation
     rc = L.he4_bench_kernel(g._h, which, reps, C.byref(ms), C.byref(byts), name, 64)
     if rc != 0:

@@ -249,8 +249,9 @@ int he4_fft_c2r(he4_handle *h, const double *in, double *out);
  * buffers), 7 the density gradient stencil, 8 the merged pot4 assembly on
  * FP64 grids, 9 the merged pot4 assembly on the float grids of the
  * FP32-convolution form, 10 the x pass C2R into a float grid, 11 the
- * density gradient into float grids (9-11 need that form; 7-11 rewrite fields of the current evaluation, so call
- * them after a field evaluation; the next step evaluates its field again).
+ * density gradient into float grids, 12 the inverse y pass (9-11 need that
+ * form; 7-11 rewrite fields of the current evaluation, so call them after a
+ * field evaluation; the next step evaluates its field again).
  * Returns the mean time per launch, the algorithmic bytes one launch moves
  * (each input read once, each output written once) and the kernel's name. */
 int he4_bench_kernel(he4_handle *h, int32_t which, int32_t reps, double *ms_per_launch,
