@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhe4b200.so")
 SOURCES = ["abi.cu", "fft.cu", "setup.cu", "field.cu", "impurity.cu", "step.cu", "energy.cu", "diag.cu", "fno.cu", "batch.cu"]
-HEADERS = ["common.cuh", "stencil.cuh", "reduce.cuh", "fft_reg.cuh", "fft_passes.cuh", "stream_stencil.cuh"]
+HEADERS = ["common.cuh", "stencil.cuh", "reduce.cuh", "fft_reg.cuh", "fft_passes.cuh", "stream_stencil.cuh", "bulk.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -37,7 +37,7 @@ def c1(pkg):
     return pkg.workloads.workload("c1")
 
 
-@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 128, 16)])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 128, 16), (128, 256, 16)])
 def test_fp32_fft_against_numpy(pkg, shape):
     import ctypes as C
     nx, ny, nz = shape

@@ -105,7 +105,7 @@ def test_vq_of_the_he2s_fci_entry(pkg, ora):
         assert np.max(np.abs(g.get_kernel("vq") - got)) > 1e-3 * np.max(np.abs(got))
 
 
-@pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 80), (48, 40, 30)])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 80), (48, 40, 30), (128, 256, 16), (256, 128, 8)])
 def test_fft_against_numpy_and_cufft(pkg, shape):
     import ctypes as C
     import torch
@@ -419,3 +419,4 @@ def test_force_xy_shared_transform(pkg, monkeypatch):
     for a, b in zip(f["1"], f["0"]):
         scale = np.max(np.abs(b))
         assert np.max(np.abs(a - b)) <= 1e-12 * scale
+
