@@ -171,30 +171,33 @@ def gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize(local)
 
-    def timed_run(g, stream):
+    def timed_run(g, stream, reps=1):
         """K PC steps from device-resident state, CUDA events on the
-        library's stream, max over ranks."""
-        g.set_state(psi, r, v)
-        # the RK-Gill starter, then one PC step of each of the 30 buffer
-        # states of the step (and at least --warmup), so every step graph is
-        # captured before timing
-        g.run(3 + max(args.warmup, 30), dt)
-        barrier()
-        n0 = g.launch_count()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
+        library's stream, max over ranks; `reps` windows, each from the same
+        state after the same warm-up, the median returned with all."""
+        windows, launches = [], 0
         with ClockSampler(local) as clk:
-            e0.record(stream)
-            err, means = g.run(args.steps, dt)
-            e1.record(stream)
-            e1.synchronize()
-        launches = g.launch_count() - n0
-        ms = e0.elapsed_time(e1)
-        barrier()
-        ms = max_over_ranks(dist, ms, f"cuda:{local}")
-        if not np.all(np.isfinite(err)) or not np.all(np.isfinite(means)):
-            raise RuntimeError("non-finite step errors in the timed region")
-        return ms, launches, clk.summary()
+            for _ in range(reps):
+                g.set_state(psi, r, v)
+                # the RK-Gill starter, then one PC step of each of the 30
+                # buffer states of the step (and at least --warmup), so every
+                # step graph is captured before timing
+                g.run(3 + max(args.warmup, 30), dt)
+                barrier()
+                n0 = g.launch_count()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                err, means = g.run(args.steps, dt)
+                e1.record(stream)
+                e1.synchronize()
+                launches = g.launch_count() - n0
+                ms = e0.elapsed_time(e1)
+                barrier()
+                windows.append(max_over_ranks(dist, ms, f"cuda:{local}"))
+                if not np.all(np.isfinite(err)) or not np.all(np.isfinite(means)):
+                    raise RuntimeError("non-finite step errors in the timed region")
+        return float(np.median(windows)), launches, clk.summary(), windows
 
     # ---- every form on the same workload; the headline is args.form
     forms = {}
@@ -206,10 +209,15 @@ def gpu_arm(args):
             continue
         gf = pkg.He4Step(form_params(pkg, p, form))
         sf = torch.cuda.ExternalStream(gf.stream(), device=torch.device("cuda", local))
-        ms_f, launches_f, clocks_f = timed_run(gf, sf)
+        # a step-form headline times exactly one window of K steps; beside the
+        # parareal headline each form is timed over --form-reps windows of K
+        # steps and the median window reported (a stall of the shared box
+        # inside one window then moves no number)
+        reps = 1 if form == args.form else max(1, args.form_reps)
+        ms_f, launches_f, clocks_f, windows = timed_run(gf, sf, reps)
         ms_step = ms_f / args.steps
         cap, unc = gf.graph_stats()
-        forms[form] = {"form": FORMS[form], "ms_per_step": ms_step,
+        forms[form] = {"form": FORMS[form], "ms_per_step": ms_step, "windows_ms": windows,
                        "value": replica_throughput(world, sim_ps, ms_f * 1e-3), "gpu_launches": launches_f,
                        "clocks": clocks_f, "graphs": {"captured": cap, "steps_uncaptured": unc}}
         # whole-step roofline: the algorithmic bytes of one PC step over its time
@@ -680,6 +688,8 @@ def main():
     ap.add_argument("--form", default="parareal", choices=sorted(FORMS))
     ap.add_argument("--fno-traj", type=int, default=200, help="training trajectories of the FNO (parareal form)")
     ap.add_argument("--fno-steps", type=int, default=1500, help="training steps of the FNO (parareal form)")
+    ap.add_argument("--form-reps", type=int, default=3,
+                    help="timed windows of K steps per step form beside the parareal headline (median reported)")
     ap.add_argument("--parareal-reps", type=int, default=3,
                     help="timed parareal runs from the same state; the median is reported")
     ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
