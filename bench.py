@@ -701,7 +701,7 @@ def main():
     ap.add_argument("--fno-steps", type=int, default=1500, help="training steps of the FNO (parareal form)")
     ap.add_argument("--form-reps", type=int, default=3,
                     help="timed windows of K steps per step form beside the parareal headline (median reported)")
-    ap.add_argument("--parareal-reps", type=int, default=3,
+    ap.add_argument("--parareal-reps", type=int, default=5,
                     help="timed parareal runs from the same state; the median is reported")
     ap.add_argument("--all-forms", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the other forms on the same workload")
