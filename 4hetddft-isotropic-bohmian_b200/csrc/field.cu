@@ -544,17 +544,20 @@ static bool split_taps(const Stencil &st, SplitTaps *tp) {
 template <typename TI, bool OTC, int M, int NX>
 static bool launch_pot4_stream(Handle *h, const TI *lin, const TI *dcg, const TI *h0, const TI *h1, const TI *h2,
                                const OtArgs &ot) {
+  constexpr bool F = std::is_same<TI, float>::value;
   using L = Pot4StreamLayout<TI, OTC, M, kStreamTY, kStreamS, NX>;
+  using LF = Pot4StreamLayout<TI, OTC, M, kStreamTY, kStreamS, NX, F>;  // centre values direct
   SplitTaps tp;
-  const bool fm = std::is_same<TI, float>::value && h->pot4_split && split_taps(h->st, &tp);
-  auto kern = fm ? k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX, std::is_same<TI, float>::value>
+  const bool fm = F && h->pot4_split && split_taps(h->st, &tp);
+  auto kern = fm ? k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX, F>
                  : k_pot4_stream<TI, OTC, M, kStreamTY, kStreamS, NX, false>;
-  const int res = stream_resident(h, kern, L::total);
+  const size_t smem = fm ? LF::total : L::total;
+  const int res = stream_resident(h, kern, smem);
   if (res == 0) return false;
   const Geo g = geo(h);
   const int yt = h->ny / kStreamTY, zc = stream_chunk(h->nz, yt, res);
-  kern<<<dim3(yt, (h->nz + zc - 1) / zc), 256, L::total, h->stream>>>(lin, h->den, dcg, h0, h1, h2, h->pot4, h->st, g,
-                                                                     ot, zc, &h->gred->err, tp);
+  kern<<<dim3(yt, (h->nz + zc - 1) / zc), 256, smem, h->stream>>>(lin, h->den, dcg, h0, h1, h2, h->pot4, h->st, g, ot,
+                                                                 zc, &h->gred->err, tp);
   HE4_LAUNCHED(h);
   return true;
 }

@@ -33,13 +33,16 @@ struct RowPad {
 
 // Shared-memory layout of one CTA (bytes), for S stages of TY rows of NX
 // points.  h0 rows (x taps) carry RowPad elements on both sides.
-template <typename TI, bool OTC, int M, int TY, int S, int NX>
+// CD (centre values direct): den, lin and dencg, which each thread reads at
+// its own points only, come straight from global memory instead of through
+// shared memory, which leaves room for a third CTA per SM.
+template <typename TI, bool OTC, int M, int TY, int S, int NX, bool CD = false>
 struct Pot4StreamLayout {
   static constexpr int RH = S + 2 * M;  // h2 ring: planes k-M .. k+M plus the S-1 in flight
   static constexpr int PX = RowPad<TI, M>::value, RS0 = NX + 2 * PX;
   static constexpr size_t rt = (size_t)NX * sizeof(TI), rd = (size_t)NX * sizeof(double);
-  static constexpr size_t bars = 0, den = 128, lin = den + (size_t)S * TY * rd, dcg = lin + (size_t)S * TY * rt,
-                          h0 = dcg + (size_t)S * TY * rt,
+  static constexpr size_t bars = 0, den = 128, lin = den + (CD ? 0 : (size_t)S * TY * rd),
+                          dcg = lin + (CD ? 0 : (size_t)S * TY * rt), h0 = dcg + (CD ? 0 : (size_t)S * TY * rt),
                           h1 = h0 + (OTC ? (size_t)S * TY * RS0 * sizeof(TI) : 0),
                           h2 = h1 + (OTC ? (size_t)S * (TY + 2 * M) * rt : 0),
                           total = h2 + (OTC ? (size_t)RH * TY * rt : 0);
@@ -72,7 +75,7 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
                                                      double *__restrict__ pot4, Stencil st, Geo g, OtArgs a, int zc,
                                                      unsigned *err, SplitTaps tp) {
   extern __shared__ __align__(128) unsigned char smem[];
-  using L = Pot4StreamLayout<TI, OTC, M, TY, S, NX>;
+  using L = Pot4StreamLayout<TI, OTC, M, TY, S, NX, FM>;
   constexpr int RH = L::RH, PX = L::PX, RS0 = L::RS0;
   constexpr unsigned rt = (unsigned)L::rt, rd = (unsigned)L::rd, pb = (unsigned)(PX * sizeof(TI));
   const int ny = g.ny, nz = g.nz;
@@ -99,16 +102,18 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
   // the copies of plane k into stage s (warp 0), plus, with `pro`, the h2
   // planes k0-M .. k0+M-1 that precede the first stage's
   auto issue = [&](int k, int s, bool pro) {
-    const unsigned bytes = TY * rd + (OTC ? (TY * (4 * rt + 2 * pb) + (TY + 2 * M) * rt + (pro ? 2 * M * TY * rt : 0))
-                                          : 2 * TY * rt);
+    const unsigned bytes = (FM ? 0 : TY * rd + 2 * TY * rt) +
+                           (OTC ? (TY * (2 * rt + 2 * pb) + (TY + 2 * M) * rt + (pro ? 2 * M * TY * rt : 0)) : 0);
     if (lane == 0) mbar_expect_tx(&bar[s], bytes);
     __syncwarp();
     const size_t pk = (size_t)k * ps;
     for (int r = lane; r < TY; r += 32) {
       const size_t o = pk + (size_t)(j0 + r) * NX;
-      bulk_row(sden + ((size_t)s * TY + r) * NX, den + o, rd, &bar[s]);
-      bulk_row(slin + ((size_t)s * TY + r) * NX, lin + o, rt, &bar[s]);
-      bulk_row(sdcg + ((size_t)s * TY + r) * NX, dencg + o, rt, &bar[s]);
+      if (!FM) {
+        bulk_row(sden + ((size_t)s * TY + r) * NX, den + o, rd, &bar[s]);
+        bulk_row(slin + ((size_t)s * TY + r) * NX, lin + o, rt, &bar[s]);
+        bulk_row(sdcg + ((size_t)s * TY + r) * NX, dencg + o, rt, &bar[s]);
+      }
       if (OTC) {
         TI *row = sh0 + ((size_t)s * TY + r) * RS0;
         bulk_row(row + PX, h0 + o, rt, &bar[s]);
@@ -135,9 +140,23 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
     for (int q = 0; q < S && k0 + q < k1; q++) issue(k0 + q, q, q == 0);
   const double a0 = a.cp4 / 2.0, a1 = a.cpp4 / 3.0, adiv = a.h2o2m4 * a.alphas;
   const float fa0 = (float)a0, fa1 = (float)a1, fcs = (float)a.c_solid, fbeta = (float)a.beta;
-  constexpr int NPT = TY * NX;
+  constexpr int NPT = TY * NX, NQ = NPT / 256;
+  static_assert(NPT % 256 == 0, "a plane's points are whole multiples of the CTA");
   for (int k = k0; k < k1; k++) {
     const int it = k - k0, s = it % S;
+    // FM: this plane's den, lin and dencg at the thread's own points, from
+    // global memory, issued before the wait so their latency overlaps it
+    double dq[FM ? NQ : 1];
+    TI lq[FM ? NQ : 1], cq[FM ? NQ : 1];
+    if constexpr (FM) {
+      const size_t b0 = (size_t)k * ps + (size_t)j0 * NX;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        dq[q] = __ldg(den + b0 + tid + 256 * q);
+        lq[q] = __ldg(lin + b0 + tid + 256 * q);
+        cq[q] = __ldg(dencg + b0 + tid + 256 * q);
+      }
+    }
     const bool ok = mbar_wait_bounded(&bar[s], (unsigned)((it / S) & 1));
     if (__syncthreads_or(!ok)) {
       // copies that did not arrive: flag, drain (bounded) what this CTA
@@ -160,14 +179,15 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
 #pragma unroll
     for (int p = tid; p < NPT; p += 256) {
       const int r = p / NX, x = p % NX;
-      const double d = dd[p];
       if constexpr (FM) {
+        const int qi = (p - tid) / 256;
+        const double d = dq[qi];
         const float xs = (float)(a.beta * (d - a.den_m)), df = (float)d;
         const float e = expf(-2.0f * fabsf(xs)), q = 1.0f / (1.0f + e);
         const float opt = (xs >= 0.0f ? 2.0f : 2.0f * e) * q, omt = 4.0f * e * q * q;
-        const float dc = cc[p];
+        const float dc = cq[qi];
         const float cp = dc * dc * (fa0 + fa1 * dc) + fcs * (opt + fbeta * df * omt);
-        double v = (double)ll[p] + (double)cp;
+        double v = (double)lq[qi] + (double)cp;
         if (OTC) {
           const TI *xr = x0 + r * RS0 + x;
           const TI *yc = y1 + r * NX + x;
@@ -188,6 +208,7 @@ __global__ void __launch_bounds__(256) k_pot4_stream(const TI *__restrict__ lin,
         out[p] = v;
         continue;
       }
+      const double d = dd[p];
       const double th = tanh(a.beta * (d - a.den_m));
       const double pen = a.c_solid * (1.0 + th + a.beta * d * (1.0 - th * th));
       const double dc = (double)cc[p];
