@@ -348,6 +348,11 @@ def parareal_form(pkg, args, p, psi, r, v, dt, local, barrier):
     pr.train(net, xs, ys, args.fno_steps, batch=2, lr=1e-3)
     after = pr.evaluate(net, hold_x, hold_y)
     t_train = time.perf_counter() - t_train
+    # the training pairs are not needed again: release them (and torch's
+    # cached blocks) before the fine handles are created and timed
+    del xs, ys, hold_x, hold_y
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     q = form_params(pkg, p, "fp32")
     coarse = pr.FnoCoarse(net, q, p.nx // spec.n, K * dt)
     par = pr.Parareal(q, S, K, dt, coarse, concurrent=8)
